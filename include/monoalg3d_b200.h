@@ -1,0 +1,256 @@
+/*
+ * monoalg3d_b200.h -- C ABI of the B200-native monodomain step.
+ *
+ * One operator-split monodomain time step of MonoAlg3D on a fixed structured
+ * mesh, run entirely on one GPU:
+ *
+ *   1. Rush-Larsen ionic ODEs (ten Tusscher 2006, ToRORd-fkatp endo/mid/epi),
+ *   2. the update_monodomain right-hand side b = alpha * V*,
+ *   3. a Jacobi-preconditioned CG solve of (alpha I + K) V = b,
+ *
+ * exactly in the order of the reference time loop
+ * (src/monodomain/monodomain_solver.c:616-925).  Every entry point takes plain
+ * pointers and sizes; host buffers are ordinary C arrays.  All functions return
+ * an int status: MB_OK (0) or one of the MB_ERR_* codes; mb_last_error()
+ * returns a readable message for the calling thread's last failure.
+ *
+ * Entry points and the reference plugin functions they replace:
+ *
+ *   mb_init_cell_model_data            init_cell_model_data
+ *                                      (src/ode_solver/ode_solver.h:33,
+ *                                       ten_tusscher_2006_RS_CPU.c:5-14,
+ *                                       ToRORd_fkatp_mixed_endo_mid_epi.c:4-10)
+ *   mb_ode_create +
+ *   mb_set_model_initial_conditions_gpu set_model_initial_conditions_gpu
+ *                                      (ode_solver.h:46; returns the pitch)
+ *   mb_solve_model_odes_gpu            solve_model_odes_gpu (ode_solver.h:37;
+ *                                      stim_currents is a host array as in
+ *                                      ode_solver.c:183-248)
+ *   mb_monodomain_create               set_initial_conditions_fvm +
+ *                                      homogeneous_sigma_assembly_matrix /
+ *                                      anisotropic_sigma_assembly_matrix
+ *                                      (matrix_assembly.c:27-45,334-514) and
+ *                                      init_conjugate_gradient
+ *                                      (linear_system_solver.c:202-216)
+ *   mb_update_monodomain_default       update_monodomain_default
+ *                                      (update_monodomain.c:19-56)
+ *   mb_conjugate_gradient              conjugate_gradient
+ *                                      (linear_system_solver.c:185-200)
+ *   mb_monodomain_step                 one pass of the solve_monodomain loop
+ *                                      body (monodomain_solver.c:616-925)
+ *   mb_csr_conjugate_gradient          cpu_conjugate_gradient /
+ *                                      gpu_conjugate_gradient on a matrix read
+ *                                      from file (test_solvers.c:28-111)
+ *   mb_monodomain_destroy              end_conjugate_gradient + free of sv
+ *
+ * Threading: every object is used from one host thread at a time, as the
+ * reference plugins are (one solver configuration per process there; one per
+ * object here).
+ */
+#ifndef MONOALG3D_B200_H
+#define MONOALG3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MB_OK               0
+#define MB_ERR_ARG          1   /* invalid argument                         */
+#define MB_ERR_CUDA         2   /* a CUDA runtime call failed               */
+#define MB_ERR_NAN          3   /* NaN in the CG error (monodomain_solver.c:746) */
+#define MB_ERR_NOMEM        4   /* host or device allocation failed         */
+#define MB_ERR_UNSUPPORTED  5   /* combination not implemented              */
+#define MB_ERR_STATE        6   /* object used in the wrong order           */
+
+/* ---- enumerations ------------------------------------------------------ */
+enum mb_model {
+    MB_MODEL_TT2006 = 0,               /* libten_tusscher_2006, 19 states    */
+    MB_MODEL_TORORD_FKATP_MIXED = 1    /* libToRORd_fkatp_mixed_endo_mid_epi, 43 states */
+};
+
+enum mb_precision {
+    MB_PREC_FP64 = 0,   /* FP64 everywhere (the plain method)                  */
+    MB_PREC_MIXED = 1   /* FP32 ODE with FP64 ion concentrations; FP32 CG with
+                           FP64 solution, FP64 dot accumulation and FP64
+                           true-residual refinement                              */
+};
+
+/* How a Rush-Larsen gate of the ToRORd model picks its branch
+ * (ToRORd_fkatp_mixed_endo_mid_epi.h:20).  The reference CPU build applies C
+ * abs() to a double, which truncates to int: every gate with |a| < 1 takes the
+ * explicit Euler branch.  MB_RL_TRUE uses |a| < 1e-8 as written.            */
+enum mb_rl_rule {
+    MB_RL_REFERENCE_CPU = 0,
+    MB_RL_TRUE = 1
+};
+
+enum mb_stim_kind {
+    MB_STIM_X_LESS_THAN = 0,   /* stim_if_x_less_than  (stimuli.c:56-91)    */
+    MB_STIM_X_Y_LIMITS = 1,    /* stim_x_y_limits      (stimuli.c:426-467)  */
+    MB_STIM_X_Y_Z_LIMITS = 2,  /* stim_x_y_z_limits    (stimuli.c:469-520)  */
+    MB_STIM_CELL_MASK = 3      /* explicit per-cell mask given by the caller */
+};
+
+enum mb_assembly {
+    /* homogeneous_sigma_assembly_matrix (matrix_assembly.c:334-387): 7-point,
+       harmonic-mean face conductivities                                     */
+    MB_ASSEMBLY_HOMOGENEOUS = 0,
+    /* anisotropic_sigma_assembly_matrix (matrix_assembly.c:389-514) with a
+       per-z-plane fibre direction in the xy plane: 19-point stencil         */
+    MB_ASSEMBLY_ANISOTROPIC = 1,
+    /* per-cell isotropic sigma, harmonic mean per face (7-point)            */
+    MB_ASSEMBLY_PER_CELL_SIGMA = 2
+};
+
+#define MB_MAX_STIMS 8
+
+typedef struct mb_stim {
+    int    kind;        /* enum mb_stim_kind                                 */
+    double start;       /* ms                                                */
+    double duration;    /* ms; active for start <= t <= start + duration     */
+    double period;      /* ms; 0 = not periodic (ode_solver.c:225-233)       */
+    double current;     /* uA/uF, added to dV/dt with a minus sign           */
+    double x_limit;     /* MB_STIM_X_LESS_THAN: center.x < x_limit (um)      */
+    double min[3];      /* MB_STIM_X_Y(_Z)_LIMITS: inclusive box on centers  */
+    double max[3];
+    const uint8_t *cell_mask; /* MB_STIM_CELL_MASK: nx*ny*nz bytes, 1 = stim */
+} mb_stim;
+
+/* Description of one tissue on a structured cuboid grid.  Cell (i,j,k) has
+ * centre ((i+1/2)dx, (j+1/2)dy, (k+1/2)dz) um, as set_cuboid_domain_mesh
+ * builds it (domain_helpers.c:19-73); grid index is i + nx*(j + ny*k).      */
+typedef struct mb_monodomain_desc {
+    int    nx, ny, nz;
+    double dx, dy, dz;                 /* um                                  */
+    const uint8_t *active;             /* nx*ny*nz bytes, 0 = removed cell;
+                                          NULL = every cell active            */
+    /* [main] */
+    double dt_pde;                     /* ms                                  */
+    double beta;                       /* 1/um   (default 0.14)               */
+    double cm;                         /* uF/cm^2 (default 1.0)               */
+    /* [ode_solver] */
+    int    model;                      /* enum mb_model                       */
+    int    precision;                  /* enum mb_precision                   */
+    int    rl_rule;                    /* enum mb_rl_rule (ToRORd only)       */
+    double dt_ode;                     /* ms; num_steps = (int)(dt_pde/dt_ode) */
+    const double *initial_state;       /* NEQ values for every cell, or NULL
+                                          for the model defaults              */
+    const uint8_t *celltype;           /* ToRORd: nx*ny*nz bytes, 0 endo,
+                                          1 mid, 2 epi; NULL = all endo       */
+    const double *current_scale;       /* per-cell conductance scalings,
+                                          MB_NUM_SCALES x (nx*ny*nz), row
+                                          major by scale; NULL = all 1        */
+    /* [assembly_matrix] */
+    int    assembly;                   /* enum mb_assembly                    */
+    double sigma[3];                   /* homogeneous: sigma_x, sigma_y, sigma_z (mS/um) */
+    double sigma_l, sigma_t, sigma_n;  /* anisotropic: along / across fibres  */
+    const double *fibre_angle_z;       /* anisotropic: nz angles (rad) of the
+                                          fibre in the xy plane, NULL = 0     */
+    const double *sigma_cell;          /* per-cell sigma (nx*ny*nz), PER_CELL */
+    /* [linear_system_solver] */
+    double cg_tolerance;               /* stop when r.r <= tolerance          */
+    int    cg_max_iterations;          /* default 200                         */
+    int    use_preconditioner;         /* Jacobi                              */
+    /* [stim_*] */
+    int    num_stims;
+    mb_stim stims[MB_MAX_STIMS];
+    /* initial transmembrane potential for the CG initial guess
+       (set_initial_conditions_fvm, matrix_assembly.c:27-45);
+       NaN = the model's INITIAL_V                                          */
+    double initial_v;
+} mb_monodomain_desc;
+
+/* Scalings of the ionic conductances, in this order (TT2006: gNa, gKr, gKs,
+ * gCaL, gK1; ToRORd: the same currents).                                    */
+#define MB_NUM_SCALES 5
+
+typedef struct mb_monodomain mb_monodomain;
+typedef struct mb_ode mb_ode;
+
+/* Per-step record kept on the device: CG iterations and final r.r. */
+typedef struct mb_step_stats {
+    int32_t cg_iterations;
+    int32_t refinements;     /* FP64 true-residual evaluations (mixed)      */
+    double  cg_error;
+} mb_step_stats;
+
+/* ---- errors / device --------------------------------------------------- */
+const char *mb_last_error(void);
+int mb_version(void);
+int mb_device_count(int *count);
+
+/* ---- cell model library (ode_solver.h:33-47) --------------------------- */
+int mb_init_cell_model_data(int model, int *number_of_ode_equations, double *initial_v);
+
+/* Stand-alone ODE object: num_cells independent cells, state in SoA rows. */
+int mb_ode_create(mb_ode **out, int model, int precision, int rl_rule,
+                  uint32_t num_cells, double dt, uint32_t num_steps);
+/* Writes the initial state; initial_state = NULL uses the model defaults,
+ * celltype = NULL makes every cell ENDO.  *pitch_out = bytes between state
+ * rows, as the reference returns from set_model_initial_conditions_gpu.    */
+int mb_set_model_initial_conditions_gpu(mb_ode *ode, const double *initial_state,
+                                        const uint8_t *celltype, size_t *pitch_out);
+/* num_steps sub-steps of size dt for every cell; stim_currents[num_cells]
+ * is read from host memory (NULL = no stimulus).                          */
+int mb_solve_model_odes_gpu(mb_ode *ode, double current_t, const double *stim_currents);
+/* Copies the state, neq rows of num_cells doubles, to host memory. */
+int mb_ode_get_state(mb_ode *ode, double *host_state);
+int mb_ode_set_state(mb_ode *ode, const double *host_state);
+void mb_ode_destroy(mb_ode *ode);
+
+/* ---- monodomain tissue ------------------------------------------------- */
+void mb_monodomain_desc_defaults(mb_monodomain_desc *d);
+int  mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *desc);
+void mb_monodomain_destroy(mb_monodomain *m);
+
+/* Runs n loop iterations of solve_monodomain (ODE, RHS, CG, clock) on the
+ * device; asynchronous with respect to the host.                          */
+int mb_monodomain_step(mb_monodomain *m, int n);
+/* Waits for the device, then checks the NaN flag. */
+int mb_monodomain_sync(mb_monodomain *m);
+
+/* The three phases one at a time, for callers that drive the loop
+ * themselves the way monodomain_solver.c does.                            */
+int mb_solve_all_volumes_odes(mb_monodomain *m);
+int mb_update_monodomain_default(mb_monodomain *m);
+int mb_conjugate_gradient(mb_monodomain *m, uint32_t *number_of_iterations, double *error);
+int mb_advance_time(mb_monodomain *m);
+
+/* Reference-host mode: per step, take the stimulus from a host array, run
+ * ODE + RHS + CG and return V to host memory -- the copies the reference GPU
+ * plugins make every step (monodomain_solver.c:1012-1105,
+ * update_monodomain.c:35-38).  stim_host may be NULL.                     */
+int mb_monodomain_step_host(mb_monodomain *m, const double *stim_host, double *v_host);
+
+/* State access (host buffers, grid order nx*ny*nz; removed cells get NaN). */
+int mb_monodomain_get_v(mb_monodomain *m, double *v_host);
+int mb_monodomain_set_v(mb_monodomain *m, const double *v_host);
+int mb_monodomain_get_state(mb_monodomain *m, double *state_host);  /* NEQ x n_active */
+int mb_monodomain_info(mb_monodomain *m, int64_t *count, double *cur_time,
+                       uint32_t *n_active, int *neq);
+int mb_monodomain_step_stats(mb_monodomain *m, int64_t first, int64_t n, mb_step_stats *out);
+/* Device pointers to V (double, grid order) and to the CUDA stream used. */
+int mb_monodomain_device_v(mb_monodomain *m, double **v_dev, void **stream);
+/* Average duration of the last kernel launches per kind, from CUDA events
+ * recorded by mb_monodomain_profile_steps: ode, cg (whole solve). */
+int mb_monodomain_profile_steps(mb_monodomain *m, int n, double *ode_ms, double *cg_ms,
+                                double *step_ms, int *cg_iterations);
+
+/* ---- general sparse CG (test_solvers.c fixtures) ---------------------- */
+/* Solves A x = b for a CSR matrix on the device; x holds the initial guess
+ * on entry.  Same iteration and stopping rule as cpu_conjugate_gradient
+ * (linear_system_solver.c:47-183).                                         */
+int mb_csr_conjugate_gradient(int32_t n, const int32_t *row_ptr, const int32_t *col,
+                              const double *val, const double *b, double *x,
+                              double tolerance, int max_iterations, int use_preconditioner,
+                              uint32_t *number_of_iterations, double *error);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MONOALG3D_B200_H */

@@ -1,0 +1,134 @@
+/* Internal layout shared by the host driver (C) and the kernels (CUDA).
+ * Nothing here is part of the public ABI. */
+#ifndef MB_INTERNAL_H
+#define MB_INTERNAL_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+#include "monoalg3d_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MB_NEQ_TT2006 19
+#define MB_NEQ_TORORD 43
+#define MB_MAX_NEQ 43
+
+/* Device-resident control block of one tissue: the loop clock, the stimulus
+ * table and the scalars of the CG recurrences.  All of the per-step control
+ * flow (stimulus windows, CG stopping rule, time advance) reads and writes
+ * this block on the device, so a captured step never returns to the host. */
+typedef struct mb_ctrl {
+    /* loop clock (monodomain_solver.c:616,907-908) */
+    double  cur_time;
+    double  final_time;
+    int64_t count;
+    /* stimuli (ode_solver.c:201-235) */
+    int32_t num_stims;
+    int32_t nan_flag;
+    double  stim_start[MB_MAX_STIMS];
+    double  stim_dur[MB_MAX_STIMS];
+    double  stim_period[MB_MAX_STIMS];
+    double  stim_current[MB_MAX_STIMS];
+    /* CG scalars (linear_system_solver.c:47-183) */
+    double  rz, rr, pq, alpha, beta;
+    double  rr_ref;          /* true r.r at the last refinement (mixed)    */
+    double  error;
+    double  tol;
+    double  refine_ratio;
+    int32_t its;
+    int32_t max_its;
+    int32_t done;
+    int32_t phase;           /* mixed: 1 = evaluate the FP64 true residual */
+    int32_t refinements;
+    int32_t use_precond;
+    uint32_t ticket;
+    uint32_t pad_;
+} mb_ctrl;
+
+/* Structured grid, device view. */
+typedef struct mb_grid_dev {
+    int32_t nx, ny, nz, pad_;
+    int64_t n;               /* nx*ny*nz                                    */
+} mb_grid_dev;
+
+/* 7-point operator (alpha I + K) on the structured grid.
+ *   kind 0: constant face coefficients cx, cy, cz; mask gives removed cells
+ *   kind 1: per-face coefficients fx, fy, fz stored at the lower cell
+ *   kind 2: 27-point rows from a class table, class = (k, xy boundary kind) */
+typedef struct mb_stencil_dev {
+    int32_t kind;
+    int32_t nx, ny, nz;
+    double  alpha;
+    double  cx, cy, cz;
+    const uint8_t *mask;      /* NULL = all active                          */
+    const double  *fx, *fy, *fz;
+    const double  *table;     /* kind 2: [nz][9][27]                        */
+    const float   *table32;   /* kind 2, FP32 copy                          */
+} mb_stencil_dev;
+
+/* ODE state, device view.  Rows of double (sv64) and float (sv32), each of
+ * length ld; compact cell t lives at column t.  V is passed separately. */
+typedef struct mb_ode_dev {
+    int32_t model, precision, rl_rule, num_steps;
+    uint32_t n;               /* cells to solve                             */
+    uint32_t ld;              /* row stride (elements)                      */
+    const uint32_t *cell;     /* compact -> grid index, NULL = identity     */
+    double *sv64;
+    float  *sv32;
+    const uint8_t *stim_bits; /* per compact cell, bit k = stim config k    */
+    const uint8_t *celltype;  /* per compact cell (ToRORd), NULL = endo     */
+    const float   *scale;     /* MB_NUM_SCALES rows of ld, NULL = 1         */
+    const double  *stim_host; /* per compact cell external stimulus, or NULL */
+    double dt;
+} mb_ode_dev;
+
+/* ---- kernel launchers (kernels.cu) ------------------------------------ */
+int mbk_ode_init(const mb_ode_dev *o, const double *table_dev, int ntypes, cudaStream_t s);
+int mbk_ode_step(const mb_ode_dev *o, mb_ctrl *ctrl, const double *vin, double *vout,
+                 cudaStream_t s);
+int mbk_ode_gather(const mb_ode_dev *o, const double *v, double *out_dev, cudaStream_t s);
+int mbk_ode_scatter(const mb_ode_dev *o, const double *in_dev, double *v, cudaStream_t s);
+
+/* CG on the structured stencil.  FP64 vectors: r, p (double).  Mixed: r32, p32. */
+typedef struct mb_cg_dev {
+    int      precision;
+    int      grid_blocks;
+    double  *x;          /* V (solution), grid order                          */
+    const double *vstar; /* V* after the ODEs; b = alpha * V*                 */
+    double  *r, *p;      /* FP64 recurrences                                  */
+    float   *r32, *p32;  /* FP32 recurrences (mixed)                          */
+    double  *partials;   /* 2 * grid_blocks                                   */
+    const double *b;     /* explicit right-hand side (CSR path) or NULL       */
+} mb_cg_dev;
+
+int mbk_cg_init(const mb_stencil_dev *st, const mb_cg_dev *cg, mb_ctrl *ctrl,
+                unsigned long long cond, int use_cond, cudaStream_t s);
+int mbk_cg_body(const mb_stencil_dev *st, const mb_cg_dev *cg, mb_ctrl *ctrl,
+                unsigned long long cond, int use_cond, cudaStream_t s);
+int mbk_step_end(mb_ctrl *ctrl, double dt_pde, double dt_ode, int num_steps,
+                 mb_step_stats *log, int64_t log_len, cudaStream_t s);
+int mbk_set_nan(double *v, const uint8_t *mask, int64_t n, cudaStream_t s);
+
+/* CSR CG (general matrices). */
+typedef struct mb_csr_dev {
+    int32_t n;
+    const int32_t *row_ptr, *col;
+    const double *val;
+    const double *b;
+    double *x, *r, *p, *q, *inv_diag;
+    double *partials;
+    int grid_blocks;
+} mb_csr_dev;
+int mbk_csr_cg_init(const mb_csr_dev *a, mb_ctrl *ctrl, cudaStream_t s);
+int mbk_csr_cg_iter(const mb_csr_dev *a, mb_ctrl *ctrl, cudaStream_t s);
+
+int mbk_max_grid_blocks(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,970 @@
+/* Host driver of the B200 monodomain step (C).
+ *
+ * Owns the device buffers of one tissue, assembles the diffusion operator,
+ * builds the per-step CUDA graph
+ *
+ *     [ ODE kernel -> CG initial residual ] -> WHILE(cond){ CG iteration } -> [ clock ]
+ *
+ * and exposes the reference's plugin entry points through the C ABI of
+ * include/monoalg3d_b200.h.  Everything in the timed loop runs on the device;
+ * the host only launches graphs.
+ */
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cuda_runtime_api.h>
+
+#include "mb_internal.h"
+#include "mb_assembly.h"
+
+/* ---- error reporting ----------------------------------------------------- */
+
+static __thread char g_err[512];
+
+static int set_err(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+const char *mb_last_error(void) { return g_err; }
+int mb_version(void) { return 10000; }
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return set_err(MB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                           __FILE__, __LINE__);                                            \
+    } while (0)
+
+#define CKK(call)                                                                          \
+    do {                                                                                   \
+        int e_ = (call);                                                                   \
+        if (e_ != 0)                                                                       \
+            return set_err(MB_ERR_CUDA, "%s failed: %s (%s:%d)", #call,                    \
+                           cudaGetErrorString((cudaError_t)e_), __FILE__, __LINE__);       \
+    } while (0)
+
+int mb_device_count(int *count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) n = 0;
+    *count = n;
+    return MB_OK;
+}
+
+/* ---- model tables -------------------------------------------------------- */
+
+int mb_init_cell_model_data(int model, int *neq, double *initial_v) {
+    if (model == MB_MODEL_TT2006) {
+        if (neq) *neq = MB_NEQ_TT2006;
+        if (initial_v) *initial_v = (double)-85.23f;          /* INITIAL_V, ten_tusscher_2006.h:7 */
+        return MB_OK;
+    }
+    if (model == MB_MODEL_TORORD_FKATP_MIXED) {
+        if (neq) *neq = MB_NEQ_TORORD;
+        if (initial_v) *initial_v = -88.763800;               /* ToRORd_fkatp_mixed_endo_mid_epi.h:11 */
+        return MB_OK;
+    }
+    return set_err(MB_ERR_ARG, "unknown model %d", model);
+}
+
+/* Row counts of the SoA state for (model, precision). */
+static void ode_rows(int model, int precision, int *n64, int *n32) {
+    if (model == MB_MODEL_TT2006) {
+        if (precision == MB_PREC_FP64) { *n64 = 19; *n32 = 0; }
+        else { *n64 = 6; *n32 = 13; }
+    } else {
+        if (precision == MB_PREC_FP64) { *n64 = 43; *n32 = 0; }
+        else { *n64 = 9; *n32 = 34; }
+    }
+}
+
+static uint32_t round_up32(uint32_t n) { return (n + 31u) & ~31u; }
+
+/* ---- standalone ODE object ---------------------------------------------- */
+
+struct mb_ode {
+    mb_ode_dev dev;
+    int neq;
+    double *d_stim;
+    cudaStream_t stream;
+};
+
+int mb_ode_create(mb_ode **out, int model, int precision, int rl_rule, uint32_t num_cells, double dt,
+                  uint32_t num_steps) {
+    if (!out || num_cells == 0 || dt <= 0.0 || num_steps == 0)
+        return set_err(MB_ERR_ARG, "mb_ode_create: bad arguments");
+    int neq;
+    if (mb_init_cell_model_data(model, &neq, NULL)) return MB_ERR_ARG;
+    if (precision != MB_PREC_FP64 && precision != MB_PREC_MIXED) return set_err(MB_ERR_ARG, "bad precision");
+    mb_ode *o = (mb_ode *)calloc(1, sizeof *o);
+    if (!o) return set_err(MB_ERR_NOMEM, "out of host memory");
+    o->neq = neq;
+    o->dev.model = model;
+    o->dev.precision = precision;
+    o->dev.rl_rule = rl_rule;
+    o->dev.num_steps = (int)num_steps;
+    o->dev.n = num_cells;
+    o->dev.ld = round_up32(num_cells);
+    o->dev.dt = dt;
+    int n64, n32;
+    ode_rows(model, precision, &n64, &n32);
+    cudaError_t e = cudaStreamCreateWithFlags(&o->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&o->dev.sv64, (size_t)n64 * o->dev.ld * sizeof(double));
+    if (e == cudaSuccess && n32) e = cudaMalloc((void **)&o->dev.sv32, (size_t)n32 * o->dev.ld * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&o->d_stim, (size_t)num_cells * sizeof(double));
+    if (e != cudaSuccess) {
+        mb_ode_destroy(o);
+        return set_err(MB_ERR_CUDA, "mb_ode_create: %s", cudaGetErrorString(e));
+    }
+    *out = o;
+    return MB_OK;
+}
+
+void mb_ode_destroy(mb_ode *o) {
+    if (!o) return;
+    cudaFree(o->dev.sv64);
+    cudaFree(o->dev.sv32);
+    cudaFree(o->d_stim);
+    if (o->stream) cudaStreamDestroy(o->stream);
+    free(o);
+}
+
+/* Initial-condition table: ntypes rows of neq doubles. */
+static int model_ic_table(int model, const double *initial_state, double *table, int *ntypes) {
+    if (model == MB_MODEL_TT2006) {
+        for (int s = 0; s < MB_NEQ_TT2006; ++s) table[s] = initial_state ? initial_state[s] : mb_tt2006_default_state(s);
+        *ntypes = 1;
+    } else {
+        if (initial_state) {
+            for (int s = 0; s < MB_NEQ_TORORD; ++s) table[s] = initial_state[s];
+            *ntypes = 1;
+        } else {
+            for (int t = 0; t < 3; ++t)
+                for (int s = 0; s < MB_NEQ_TORORD; ++s) table[t * MB_NEQ_TORORD + s] = mb_torord_default_state(t, s);
+            *ntypes = 3;
+        }
+    }
+    return MB_OK;
+}
+
+int mb_set_model_initial_conditions_gpu(mb_ode *o, const double *initial_state, const uint8_t *celltype,
+                                        size_t *pitch_out) {
+    if (!o) return set_err(MB_ERR_ARG, "null ode");
+    double table[3 * MB_MAX_NEQ];
+    int ntypes;
+    model_ic_table(o->dev.model, initial_state, table, &ntypes);
+    double *d_table = NULL;
+    uint8_t *d_ct = NULL;
+    CK(cudaMalloc((void **)&d_table, sizeof table));
+    CK(cudaMemcpyAsync(d_table, table, sizeof table, cudaMemcpyHostToDevice, o->stream));
+    mb_ode_dev dv = o->dev;
+    if (celltype && ntypes > 1) {
+        CK(cudaMalloc((void **)&d_ct, o->dev.n));
+        CK(cudaMemcpyAsync(d_ct, celltype, o->dev.n, cudaMemcpyHostToDevice, o->stream));
+        dv.celltype = d_ct;
+    }
+    CKK(mbk_ode_init(&dv, d_table, ntypes, o->stream));
+    CK(cudaStreamSynchronize(o->stream));
+    cudaFree(d_table);
+    if (d_ct) {
+        /* keep the cell types for the solve calls */
+        if (o->dev.celltype) cudaFree((void *)o->dev.celltype);
+        o->dev.celltype = d_ct;
+    }
+    if (pitch_out) *pitch_out = (size_t)o->dev.ld * sizeof(double);
+    return MB_OK;
+}
+
+int mb_solve_model_odes_gpu(mb_ode *o, double current_t, const double *stim_currents) {
+    (void)current_t;
+    if (!o) return set_err(MB_ERR_ARG, "null ode");
+    mb_ode_dev dv = o->dev;
+    if (stim_currents) {
+        CK(cudaMemcpyAsync(o->d_stim, stim_currents, (size_t)o->dev.n * sizeof(double), cudaMemcpyHostToDevice,
+                           o->stream));
+    } else {
+        CK(cudaMemsetAsync(o->d_stim, 0, (size_t)o->dev.n * sizeof(double), o->stream));
+    }
+    dv.stim_host = o->d_stim;
+    /* V lives in row 0 of the double rows: read and written in place */
+    CKK(mbk_ode_step(&dv, NULL, dv.sv64, dv.sv64, o->stream));
+    CK(cudaStreamSynchronize(o->stream));
+    return MB_OK;
+}
+
+int mb_ode_get_state(mb_ode *o, double *host_state) {
+    if (!o || !host_state) return set_err(MB_ERR_ARG, "null argument");
+    double *d = NULL;
+    const size_t bytes = (size_t)o->neq * o->dev.n * sizeof(double);
+    CK(cudaMalloc((void **)&d, bytes));
+    CKK(mbk_ode_gather(&o->dev, NULL, d, o->stream));
+    CK(cudaMemcpyAsync(host_state, d, bytes, cudaMemcpyDeviceToHost, o->stream));
+    CK(cudaStreamSynchronize(o->stream));
+    cudaFree(d);
+    return MB_OK;
+}
+
+int mb_ode_set_state(mb_ode *o, const double *host_state) {
+    if (!o || !host_state) return set_err(MB_ERR_ARG, "null argument");
+    double *d = NULL;
+    const size_t bytes = (size_t)o->neq * o->dev.n * sizeof(double);
+    CK(cudaMalloc((void **)&d, bytes));
+    CK(cudaMemcpyAsync(d, host_state, bytes, cudaMemcpyHostToDevice, o->stream));
+    CKK(mbk_ode_scatter(&o->dev, d, NULL, o->stream));
+    CK(cudaStreamSynchronize(o->stream));
+    cudaFree(d);
+    return MB_OK;
+}
+
+/* ---- monodomain tissue --------------------------------------------------- */
+
+struct mb_monodomain {
+    mb_monodomain_desc desc;
+    int neq;
+    int num_steps;
+    int64_t n;            /* grid cells */
+    uint32_t n_active;
+    cudaStream_t stream;
+
+    uint8_t *d_mask;
+    uint32_t *d_cells;
+    double *d_v, *d_vstar;
+    double *d_r, *d_p;
+    float *d_r32, *d_p32;
+    double *d_partials;
+    double *d_sv64;
+    float *d_sv32;
+    uint8_t *d_stim_bits;
+    uint8_t *d_celltype;
+    float *d_scale;
+    double *d_fx, *d_fy, *d_fz;
+    double *d_table;
+    float *d_table32;
+    double *d_stim_host;
+    mb_ctrl *d_ctrl;
+    mb_step_stats *d_log;
+    int64_t log_len;
+    uint8_t *h_mask;      /* owned copy of desc.active (NULL = all active) */
+
+    mb_ode_dev ode;
+    mb_stencil_dev st;
+    mb_cg_dev cg;
+
+    cudaGraph_t g_pre, g_body_owner_unused, g_post;
+    cudaGraph_t g_step;
+    cudaGraphExec_t ge_step;
+    cudaGraph_t g_cg;
+    cudaGraphExec_t ge_cg;
+    int use_graphs;
+    int phase;            /* split-API state: 0 idle, 1 ODE done, 2 RHS formed */
+    cudaEvent_t ev[4];
+};
+
+void mb_monodomain_desc_defaults(mb_monodomain_desc *d) {
+    memset(d, 0, sizeof *d);
+    d->dx = d->dy = d->dz = 100.0;
+    d->dt_pde = 0.02;
+    d->dt_ode = 0.02;
+    d->beta = 0.14;
+    d->cm = 1.0;
+    d->model = MB_MODEL_TT2006;
+    d->precision = MB_PREC_FP64;
+    d->rl_rule = MB_RL_REFERENCE_CPU;
+    d->assembly = MB_ASSEMBLY_HOMOGENEOUS;
+    d->sigma[0] = d->sigma[1] = d->sigma[2] = 0.00013;
+    d->cg_tolerance = 1e-16;
+    d->cg_max_iterations = 200;
+    d->use_preconditioner = 1;
+    d->initial_v = NAN;
+}
+
+/* alpha = ((beta * cm) / dt) * UM2_TO_CM2 * (dx dy dz), with UM2_TO_CM2 the
+ * float literal 1e-8f (monodomain/constants.h:10-11). */
+double mb_alpha(double beta, double cm, double dt, double dx, double dy, double dz) {
+    return (((beta * cm) / dt) * (double)0.00000001f) * ((dx * dy) * dz);
+}
+
+static void destroy_graphs(mb_monodomain *m) {
+    if (m->ge_step) cudaGraphExecDestroy(m->ge_step);
+    if (m->g_step) cudaGraphDestroy(m->g_step);
+    if (m->ge_cg) cudaGraphExecDestroy(m->ge_cg);
+    if (m->g_cg) cudaGraphDestroy(m->g_cg);
+    m->ge_step = NULL; m->g_step = NULL; m->ge_cg = NULL; m->g_cg = NULL;
+}
+
+void mb_monodomain_destroy(mb_monodomain *m) {
+    if (!m) return;
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    destroy_graphs(m);
+    void *bufs[] = {m->d_mask, m->d_cells, m->d_v, m->d_vstar, m->d_r, m->d_p, m->d_r32, m->d_p32,
+                    m->d_partials, m->d_sv64, m->d_sv32, m->d_stim_bits, m->d_celltype, m->d_scale,
+                    m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_stim_host, m->d_ctrl, m->d_log};
+    for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
+    for (int i = 0; i < 4; ++i) if (m->ev[i]) cudaEventDestroy(m->ev[i]);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    free(m->h_mask);
+    free(m);
+}
+
+/* Does stim config s cover the cell with centre c?  Same comparisons as the
+ * reference stimulus functions. */
+static int stim_covers(const mb_stim *s, const double c[3], int64_t g) {
+    switch (s->kind) {
+    case MB_STIM_X_LESS_THAN: return c[0] < s->x_limit;                       /* stimuli.c:82 */
+    case MB_STIM_X_Y_LIMITS:                                                    /* stimuli.c:455-456 */
+        return (c[0] >= s->min[0]) && (c[0] <= s->max[0]) && (c[1] >= s->min[1]) && (c[1] <= s->max[1]);
+    case MB_STIM_X_Y_Z_LIMITS:                                                  /* stimuli.c:505-507 */
+        return (c[0] >= s->min[0]) && (c[0] <= s->max[0]) && (c[1] >= s->min[1]) && (c[1] <= s->max[1]) &&
+               (c[2] >= s->min[2]) && (c[2] <= s->max[2]);
+    case MB_STIM_CELL_MASK: return s->cell_mask ? s->cell_mask[g] != 0 : 0;
+    default: return 0;
+    }
+}
+
+#define ALLOC(ptr, bytes)                                                                  \
+    do {                                                                                   \
+        cudaError_t e_ = cudaMalloc((void **)&(ptr), (bytes));                             \
+        if (e_ != cudaSuccess) {                                                           \
+            rc = set_err(MB_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", (size_t)(bytes),      \
+                         cudaGetErrorString(e_));                                          \
+            goto fail;                                                                     \
+        }                                                                                  \
+    } while (0)
+
+#define UPLOAD(dst, src, bytes)                                                            \
+    do {                                                                                   \
+        cudaError_t e_ = cudaMemcpy((dst), (src), (bytes), cudaMemcpyHostToDevice);        \
+        if (e_ != cudaSuccess) {                                                           \
+            rc = set_err(MB_ERR_CUDA, "cudaMemcpy failed: %s", cudaGetErrorString(e_));    \
+            goto fail;                                                                     \
+        }                                                                                  \
+    } while (0)
+
+static int build_graphs(mb_monodomain *m);
+
+int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
+    int rc = MB_OK;
+    uint32_t *cells = NULL;
+    uint8_t *bits = NULL, *ct = NULL;
+    float *scale = NULL;
+    double *vinit = NULL;
+    mb_assembly_out asmb;
+    memset(&asmb, 0, sizeof asmb);
+    if (!out || !d) return set_err(MB_ERR_ARG, "null argument");
+    *out = NULL;
+    if (d->nx <= 0 || d->ny <= 0 || d->nz <= 0) return set_err(MB_ERR_ARG, "grid dimensions must be positive");
+    if (!(d->dx > 0 && d->dy > 0 && d->dz > 0 && d->dt_pde > 0 && d->dt_ode > 0))
+        return set_err(MB_ERR_ARG, "dx, dy, dz, dt_pde and dt_ode must be positive");
+    if (d->num_stims < 0 || d->num_stims > MB_MAX_STIMS) return set_err(MB_ERR_ARG, "num_stims out of range");
+    if (d->precision != MB_PREC_FP64 && d->precision != MB_PREC_MIXED) return set_err(MB_ERR_ARG, "bad precision");
+    int neq;
+    double model_v0;
+    if (mb_init_cell_model_data(d->model, &neq, &model_v0)) return MB_ERR_ARG;
+    const int64_t n = (int64_t)d->nx * d->ny * d->nz;
+    if (n > 0x7fffffffLL) return set_err(MB_ERR_ARG, "grid too large (%lld cells)", (long long)n);
+
+    mb_monodomain *m = (mb_monodomain *)calloc(1, sizeof *m);
+    if (!m) return set_err(MB_ERR_NOMEM, "out of host memory");
+    m->desc = *d;
+    m->neq = neq;
+    m->n = n;
+    m->use_graphs = getenv("MB_NO_GRAPH") == NULL;
+    /* num_steps = (int)(dt_pde / dt_ode) (monodomain_solver.c:510-520) */
+    m->num_steps = d->dt_pde >= d->dt_ode ? (int)(d->dt_pde / d->dt_ode) : 1;
+    if (m->num_steps < 1) m->num_steps = 1;
+
+    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        rc = set_err(MB_ERR_CUDA, "cudaStreamCreate failed");
+        goto fail;
+    }
+    for (int i = 0; i < 4; ++i) cudaEventCreate(&m->ev[i]);
+
+    /* active cells, compact numbering in grid order */
+    uint32_t na = 0;
+    if (d->active) {
+        cells = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+        if (!cells) { rc = set_err(MB_ERR_NOMEM, "host memory"); goto fail; }
+        for (int64_t g = 0; g < n; ++g) if (d->active[g]) cells[na++] = (uint32_t)g;
+    } else {
+        na = (uint32_t)n;
+    }
+    m->n_active = na;
+    if (na == 0) { rc = set_err(MB_ERR_ARG, "no active cells"); goto fail; }
+    const uint32_t ld = round_up32(na);
+
+    /* ODE state */
+    int n64, n32;
+    ode_rows(d->model, d->precision, &n64, &n32);
+    ALLOC(m->d_sv64, (size_t)n64 * ld * sizeof(double));
+    if (n32) ALLOC(m->d_sv32, (size_t)n32 * ld * sizeof(float));
+    m->ode.model = d->model;
+    m->ode.precision = d->precision;
+    m->ode.rl_rule = d->rl_rule;
+    m->ode.num_steps = m->num_steps;
+    m->ode.n = na;
+    m->ode.ld = ld;
+    m->ode.sv64 = m->d_sv64;
+    m->ode.sv32 = m->d_sv32;
+    m->ode.dt = d->dt_ode;
+    if (d->active) {
+        ALLOC(m->d_mask, (size_t)n);
+        UPLOAD(m->d_mask, d->active, (size_t)n);
+        ALLOC(m->d_cells, (size_t)na * sizeof(uint32_t));
+        UPLOAD(m->d_cells, cells, (size_t)na * sizeof(uint32_t));
+        m->ode.cell = m->d_cells;
+    }
+
+    /* stimulus bits per compact cell */
+    if (d->num_stims > 0) {
+        bits = (uint8_t *)calloc(na, 1);
+        if (!bits) { rc = set_err(MB_ERR_NOMEM, "host memory"); goto fail; }
+        int any = 0;
+        for (uint32_t t = 0; t < na; ++t) {
+            const int64_t g = cells ? cells[t] : t;
+            const int i = (int)(g % d->nx), j = (int)((g / d->nx) % d->ny), k = (int)(g / ((int64_t)d->nx * d->ny));
+            const double c[3] = {(i + 0.5) * d->dx, (j + 0.5) * d->dy, (k + 0.5) * d->dz};
+            for (int s = 0; s < d->num_stims; ++s)
+                if (stim_covers(&d->stims[s], c, g)) { bits[t] |= (uint8_t)(1u << s); any = 1; }
+        }
+        if (any) {
+            ALLOC(m->d_stim_bits, na);
+            UPLOAD(m->d_stim_bits, bits, na);
+            m->ode.stim_bits = m->d_stim_bits;
+        }
+    }
+    ALLOC(m->d_stim_host, (size_t)na * sizeof(double));
+
+    /* cell types (ToRORd transmurality) and conductance scalings, compacted */
+    if (d->celltype && d->model == MB_MODEL_TORORD_FKATP_MIXED) {
+        ct = (uint8_t *)malloc(na);
+        if (!ct) { rc = set_err(MB_ERR_NOMEM, "host memory"); goto fail; }
+        for (uint32_t t = 0; t < na; ++t) ct[t] = d->celltype[cells ? cells[t] : t];
+        ALLOC(m->d_celltype, na);
+        UPLOAD(m->d_celltype, ct, na);
+        m->ode.celltype = m->d_celltype;
+    }
+    if (d->current_scale) {
+        scale = (float *)calloc((size_t)MB_NUM_SCALES * ld, sizeof(float));
+        if (!scale) { rc = set_err(MB_ERR_NOMEM, "host memory"); goto fail; }
+        for (int q = 0; q < MB_NUM_SCALES; ++q)
+            for (uint32_t t = 0; t < na; ++t) scale[(size_t)q * ld + t] = (float)d->current_scale[(size_t)q * n + (cells ? cells[t] : t)];
+        ALLOC(m->d_scale, (size_t)MB_NUM_SCALES * ld * sizeof(float));
+        UPLOAD(m->d_scale, scale, (size_t)MB_NUM_SCALES * ld * sizeof(float));
+        m->ode.scale = m->d_scale;
+    }
+
+    /* initial conditions of the ODE state */
+    {
+        double table[3 * MB_MAX_NEQ];
+        int ntypes;
+        model_ic_table(d->model, d->initial_state, table, &ntypes);
+        double *d_table = NULL;
+        ALLOC(d_table, sizeof table);
+        UPLOAD(d_table, table, sizeof table);
+        int e = mbk_ode_init(&m->ode, d_table, ntypes, m->stream);
+        cudaStreamSynchronize(m->stream);
+        cudaFree(d_table);
+        if (e) { rc = set_err(MB_ERR_CUDA, "ode init: %s", cudaGetErrorString((cudaError_t)e)); goto fail; }
+    }
+
+    /* V (grid): the CG initial guess is the assembly init value
+     * (set_initial_conditions_fvm); V* starts at the ODE state's own V so that
+     * the first ODE step reads sv[0] (update_ode_state_vector is skipped at t = 0). */
+    ALLOC(m->d_v, (size_t)n * sizeof(double));
+    ALLOC(m->d_vstar, (size_t)n * sizeof(double));
+    {
+        const double v0 = isnan(d->initial_v) ? model_v0 : d->initial_v;
+        vinit = (double *)malloc((size_t)n * sizeof(double));
+        if (!vinit) { rc = set_err(MB_ERR_NOMEM, "host memory"); goto fail; }
+        for (int64_t g = 0; g < n; ++g) vinit[g] = (!d->active || d->active[g]) ? v0 : 0.0;
+        UPLOAD(m->d_v, vinit, (size_t)n * sizeof(double));
+        CKK(cudaMemset(m->d_vstar, 0, (size_t)n * sizeof(double)));
+        /* V* <- state V (row 0 of the ODE table rows) */
+        double *dense = NULL;
+        ALLOC(dense, (size_t)neq * na * sizeof(double));
+        mbk_ode_gather(&m->ode, NULL, dense, m->stream);
+        mb_ode_dev tmp = m->ode;
+        int e = mbk_ode_scatter(&tmp, dense, m->d_vstar, m->stream);
+        cudaStreamSynchronize(m->stream);
+        cudaFree(dense);
+        if (e) { rc = set_err(MB_ERR_CUDA, "V* init failed"); goto fail; }
+    }
+
+    /* diffusion operator */
+    m->st.nx = d->nx; m->st.ny = d->ny; m->st.nz = d->nz;
+    m->st.alpha = mb_alpha(d->beta, d->cm, d->dt_pde, d->dx, d->dy, d->dz);
+    m->st.mask = m->d_mask;
+    rc = mb_assemble(d, &asmb);
+    if (rc) goto fail;
+    m->st.kind = asmb.kind;
+    m->st.cx = asmb.cx; m->st.cy = asmb.cy; m->st.cz = asmb.cz;
+    if (asmb.kind == 1) {
+        ALLOC(m->d_fx, (size_t)n * sizeof(double));
+        ALLOC(m->d_fy, (size_t)n * sizeof(double));
+        ALLOC(m->d_fz, (size_t)n * sizeof(double));
+        UPLOAD(m->d_fx, asmb.fx, (size_t)n * sizeof(double));
+        UPLOAD(m->d_fy, asmb.fy, (size_t)n * sizeof(double));
+        UPLOAD(m->d_fz, asmb.fz, (size_t)n * sizeof(double));
+        m->st.fx = m->d_fx; m->st.fy = m->d_fy; m->st.fz = m->d_fz;
+    } else if (asmb.kind == 2) {
+        const size_t tn = (size_t)d->nz * 9 * 27;
+        ALLOC(m->d_table, tn * sizeof(double));
+        UPLOAD(m->d_table, asmb.table, tn * sizeof(double));
+        float *t32 = (float *)malloc(tn * sizeof(float));
+        if (!t32) { rc = set_err(MB_ERR_NOMEM, "host memory"); goto fail; }
+        for (size_t q = 0; q < tn; ++q) t32[q] = (float)asmb.table[q];
+        ALLOC(m->d_table32, tn * sizeof(float));
+        cudaMemcpy(m->d_table32, t32, tn * sizeof(float), cudaMemcpyHostToDevice);
+        free(t32);
+        m->st.table = m->d_table; m->st.table32 = m->d_table32;
+    }
+
+    /* CG work vectors */
+    m->cg.precision = d->precision;
+    {
+        int gb = (int)((n + 255) / 256);
+        if (gb > mbk_max_grid_blocks()) gb = mbk_max_grid_blocks();
+        if (gb < 1) gb = 1;
+        m->cg.grid_blocks = gb;
+        ALLOC(m->d_partials, (size_t)3 * gb * sizeof(double));
+    }
+    if (d->precision == MB_PREC_FP64) {
+        ALLOC(m->d_r, (size_t)n * sizeof(double));
+        ALLOC(m->d_p, (size_t)n * sizeof(double));
+        CKK(cudaMemset(m->d_r, 0, (size_t)n * sizeof(double)));
+        CKK(cudaMemset(m->d_p, 0, (size_t)n * sizeof(double)));
+    } else {
+        ALLOC(m->d_r32, (size_t)n * sizeof(float));
+        ALLOC(m->d_p32, (size_t)n * sizeof(float));
+        CKK(cudaMemset(m->d_r32, 0, (size_t)n * sizeof(float)));
+        CKK(cudaMemset(m->d_p32, 0, (size_t)n * sizeof(float)));
+    }
+    m->cg.x = m->d_v;
+    m->cg.vstar = m->d_vstar;
+    m->cg.r = m->d_r; m->cg.p = m->d_p;
+    m->cg.r32 = m->d_r32; m->cg.p32 = m->d_p32;
+    m->cg.partials = m->d_partials;
+
+    /* control block */
+    {
+        mb_ctrl c;
+        memset(&c, 0, sizeof c);
+        c.cur_time = 0.0;
+        c.count = 0;
+        c.num_stims = d->num_stims;
+        for (int s = 0; s < d->num_stims; ++s) {
+            c.stim_start[s] = d->stims[s].start;
+            c.stim_dur[s] = d->stims[s].duration;
+            c.stim_period[s] = d->stims[s].period;
+            c.stim_current[s] = d->stims[s].current;
+        }
+        c.tol = d->cg_tolerance;
+        c.max_its = d->cg_max_iterations > 0 ? d->cg_max_iterations : 200;
+        c.use_precond = d->use_preconditioner ? 1 : 0;
+        c.refine_ratio = 1e-8;
+        ALLOC(m->d_ctrl, sizeof(mb_ctrl));
+        UPLOAD(m->d_ctrl, &c, sizeof c);
+    }
+    m->log_len = 1 << 20;
+    ALLOC(m->d_log, (size_t)m->log_len * sizeof(mb_step_stats));
+
+    rc = build_graphs(m);
+    if (rc) goto fail;
+
+    free(cells); free(bits); free(ct); free(scale); free(vinit);
+    mb_assembly_free(&asmb);
+    /* keep no caller pointers beyond this call */
+    if (d->active) {
+        m->h_mask = (uint8_t *)malloc((size_t)n);
+        if (!m->h_mask) { mb_monodomain_destroy(m); return set_err(MB_ERR_NOMEM, "host memory"); }
+        memcpy(m->h_mask, d->active, (size_t)n);
+    }
+    m->desc.active = m->h_mask;
+    m->desc.initial_state = NULL;
+    m->desc.celltype = NULL;
+    m->desc.current_scale = NULL;
+    m->desc.fibre_angle_z = NULL;
+    m->desc.sigma_cell = NULL;
+    for (int s = 0; s < MB_MAX_STIMS; ++s) m->desc.stims[s].cell_mask = NULL;
+    *out = m;
+    return MB_OK;
+fail:
+    free(cells); free(bits); free(ct); free(scale); free(vinit);
+    mb_assembly_free(&asmb);
+    mb_monodomain_destroy(m);
+    return rc ? rc : MB_ERR_CUDA;
+}
+
+/* Captures the launches of fn into a fresh graph. */
+typedef int (*capture_fn)(mb_monodomain *m, int in_body);
+
+static int cap_pre(mb_monodomain *m, int in_body) {
+    (void)in_body;
+    int e = mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream);
+    if (!e) e = mbk_cg_init(&m->st, &m->cg, m->d_ctrl, 0ULL, 0, m->stream);
+    return e;
+}
+
+static int cap_cginit(mb_monodomain *m, int in_body) {
+    (void)in_body;
+    return mbk_cg_init(&m->st, &m->cg, m->d_ctrl, 0ULL, 0, m->stream);
+}
+
+static int cap_post(mb_monodomain *m, int in_body) {
+    (void)in_body;
+    return mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream);
+}
+
+static unsigned long long g_cond_handle;
+
+static int cap_body(mb_monodomain *m, int in_body) {
+    (void)in_body;
+    return mbk_cg_body(&m->st, &m->cg, m->d_ctrl, g_cond_handle, 1, m->stream);
+}
+
+static int capture_graph(mb_monodomain *m, capture_fn fn, cudaGraph_t *out) {
+    CK(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+    int e = fn(m, 0);
+    cudaGraph_t g = NULL;
+    cudaError_t ee = cudaStreamEndCapture(m->stream, &g);
+    if (e) return set_err(MB_ERR_CUDA, "launch during capture failed: %s", cudaGetErrorString((cudaError_t)e));
+    if (ee != cudaSuccess) return set_err(MB_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(ee));
+    *out = g;
+    return MB_OK;
+}
+
+/* graph = [child pre] -> WHILE(cond){ body } -> [child post]  (post optional) */
+static int build_loop_graph(mb_monodomain *m, capture_fn pre, capture_fn post, cudaGraph_t *out,
+                            cudaGraphExec_t *exec_out) {
+    cudaGraph_t g = NULL, gpre = NULL, gpost = NULL;
+    CK(cudaGraphCreate(&g, 0));
+    int rc = capture_graph(m, pre, &gpre);
+    if (rc) return rc;
+    cudaGraphNode_t npre, ncond, npost;
+    CK(cudaGraphAddChildGraphNode(&npre, g, NULL, 0, gpre));
+    cudaGraphDestroy(gpre);
+
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    struct cudaGraphNodeParams cp;
+    memset(&cp, 0, sizeof cp);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    CK(cudaGraphAddNode(&ncond, g, &npre, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    g_cond_handle = (unsigned long long)h;
+    CK(cudaStreamBeginCaptureToGraph(m->stream, body, NULL, NULL, 0, cudaStreamCaptureModeThreadLocal));
+    int e = cap_body(m, 1);
+    cudaGraph_t body_out = NULL;
+    cudaError_t ee = cudaStreamEndCapture(m->stream, &body_out);
+    if (e) return set_err(MB_ERR_CUDA, "CG body capture failed: %s", cudaGetErrorString((cudaError_t)e));
+    if (ee != cudaSuccess) return set_err(MB_ERR_CUDA, "CG body capture: %s", cudaGetErrorString(ee));
+
+    if (post) {
+        rc = capture_graph(m, post, &gpost);
+        if (rc) return rc;
+        CK(cudaGraphAddChildGraphNode(&npost, g, &ncond, 1, gpost));
+        cudaGraphDestroy(gpost);
+    }
+    CK(cudaGraphInstantiate(exec_out, g, 0));
+    *out = g;
+    return MB_OK;
+}
+
+static int build_graphs(mb_monodomain *m) {
+    if (!m->use_graphs) return MB_OK;
+    int rc = build_loop_graph(m, cap_pre, cap_post, &m->g_step, &m->ge_step);
+    if (!rc) rc = build_loop_graph(m, cap_cginit, NULL, &m->g_cg, &m->ge_cg);
+    if (rc) {
+        /* fall back to host-driven launches */
+        cudaGetLastError();
+        destroy_graphs(m);
+        m->use_graphs = 0;
+        if (getenv("MB_REQUIRE_GRAPH")) return rc;
+    }
+    return MB_OK;
+}
+
+int mb_monodomain_uses_graphs(mb_monodomain *m) { return m ? m->use_graphs : 0; }
+
+/* Host-driven CG loop (no conditional graph): iterations in chunks, the
+ * stopping flag read back between chunks. */
+static int cg_host_loop(mb_monodomain *m) {
+    CKK(mbk_cg_init(&m->st, &m->cg, m->d_ctrl, 0ULL, 0, m->stream));
+    const int chunk = 8;
+    for (int it = 0; it < m->desc.cg_max_iterations + 2; it += chunk) {
+        for (int q = 0; q < chunk; ++q) CKK(mbk_cg_body(&m->st, &m->cg, m->d_ctrl, 0ULL, 0, m->stream));
+        int32_t done = 0;
+        CK(cudaMemcpyAsync(&done, &m->d_ctrl->done, sizeof done, cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+        if (done) break;
+    }
+    return MB_OK;
+}
+
+static int step_once(mb_monodomain *m) {
+    if (m->use_graphs) {
+        CK(cudaGraphLaunch(m->ge_step, m->stream));
+        return MB_OK;
+    }
+    CKK(mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
+    int rc = cg_host_loop(m);
+    if (rc) return rc;
+    CKK(mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream));
+    return MB_OK;
+}
+
+int mb_monodomain_step(mb_monodomain *m, int n) {
+    if (!m || n < 0) return set_err(MB_ERR_ARG, "bad arguments");
+    if (m->phase != 0) return set_err(MB_ERR_STATE, "a split step is in progress");
+    for (int i = 0; i < n; ++i) {
+        int rc = step_once(m);
+        if (rc) return rc;
+    }
+    return MB_OK;
+}
+
+int mb_monodomain_sync(mb_monodomain *m) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    CK(cudaStreamSynchronize(m->stream));
+    int32_t nan_flag = 0;
+    CK(cudaMemcpy(&nan_flag, &m->d_ctrl->nan_flag, sizeof nan_flag, cudaMemcpyDeviceToHost));
+    if (nan_flag) return set_err(MB_ERR_NAN, "NaN in the CG error: the cell model diverged");
+    return MB_OK;
+}
+
+/* ---- split API (the reference loop body one call at a time) ------------- */
+
+int mb_solve_all_volumes_odes(mb_monodomain *m) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    if (m->phase != 0) return set_err(MB_ERR_STATE, "ODE step already taken for this time step");
+    CKK(mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
+    m->phase = 1;
+    return MB_OK;
+}
+
+/* b = alpha V* is formed inside the first CG kernel; this call only checks
+ * the order of the phases. */
+int mb_update_monodomain_default(mb_monodomain *m) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    if (m->phase != 1) return set_err(MB_ERR_STATE, "update_monodomain before the ODE step");
+    m->phase = 2;
+    return MB_OK;
+}
+
+int mb_conjugate_gradient(mb_monodomain *m, uint32_t *its, double *error) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    if (m->phase != 2) return set_err(MB_ERR_STATE, "conjugate_gradient before update_monodomain");
+    if (m->use_graphs) {
+        CK(cudaGraphLaunch(m->ge_cg, m->stream));
+    } else {
+        int rc = cg_host_loop(m);
+        if (rc) return rc;
+    }
+    mb_ctrl c;
+    CK(cudaMemcpyAsync(&c, m->d_ctrl, sizeof c, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    if (its) *its = (uint32_t)c.its;
+    if (error) *error = c.error;
+    m->phase = 3;
+    return MB_OK;
+}
+
+int mb_advance_time(mb_monodomain *m) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    if (m->phase != 3) return set_err(MB_ERR_STATE, "advance_time before conjugate_gradient");
+    CKK(mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream));
+    m->phase = 0;
+    return MB_OK;
+}
+
+int mb_monodomain_step_host(mb_monodomain *m, const double *stim_host, double *v_host) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    mb_ode_dev o = m->ode;
+    if (stim_host) {
+        CK(cudaMemcpyAsync(m->d_stim_host, stim_host, (size_t)m->n_active * sizeof(double), cudaMemcpyHostToDevice,
+                           m->stream));
+        o.stim_host = m->d_stim_host;
+    }
+    CKK(mbk_ode_step(&o, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
+    if (m->use_graphs) {
+        CK(cudaGraphLaunch(m->ge_cg, m->stream));
+    } else {
+        int rc = cg_host_loop(m);
+        if (rc) return rc;
+    }
+    CKK(mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream));
+    if (v_host) {
+        CK(cudaMemcpyAsync(v_host, m->d_v, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+    }
+    return MB_OK;
+}
+
+/* ---- state access --------------------------------------------------------- */
+
+int mb_monodomain_get_v(mb_monodomain *m, double *v_host) {
+    if (!m || !v_host) return set_err(MB_ERR_ARG, "null");
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaMemcpy(v_host, m->d_v, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (m->desc.active)
+        for (int64_t g = 0; g < m->n; ++g) if (!m->desc.active[g]) v_host[g] = NAN;
+    return MB_OK;
+}
+
+int mb_monodomain_set_v(mb_monodomain *m, const double *v_host) {
+    if (!m || !v_host) return set_err(MB_ERR_ARG, "null");
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaMemcpy(m->d_v, v_host, (size_t)m->n * sizeof(double), cudaMemcpyHostToDevice));
+    return MB_OK;
+}
+
+int mb_monodomain_get_state(mb_monodomain *m, double *state_host) {
+    if (!m || !state_host) return set_err(MB_ERR_ARG, "null");
+    double *d = NULL;
+    const size_t bytes = (size_t)m->neq * m->n_active * sizeof(double);
+    CK(cudaMalloc((void **)&d, bytes));
+    /* V of the state is the grid V (after the CG) */
+    CKK(mbk_ode_gather(&m->ode, m->d_v, d, m->stream));
+    CK(cudaMemcpyAsync(state_host, d, bytes, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    cudaFree(d);
+    return MB_OK;
+}
+
+int mb_monodomain_info(mb_monodomain *m, int64_t *count, double *cur_time, uint32_t *n_active, int *neq) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    mb_ctrl c;
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaMemcpy(&c, m->d_ctrl, sizeof c, cudaMemcpyDeviceToHost));
+    if (count) *count = c.count;
+    if (cur_time) *cur_time = c.cur_time;
+    if (n_active) *n_active = m->n_active;
+    if (neq) *neq = m->neq;
+    return MB_OK;
+}
+
+int mb_monodomain_step_stats(mb_monodomain *m, int64_t first, int64_t n, mb_step_stats *out) {
+    if (!m || !out || first < 0 || n < 0 || first + n > m->log_len) return set_err(MB_ERR_ARG, "bad range");
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaMemcpy(out, m->d_log + first, (size_t)n * sizeof(mb_step_stats), cudaMemcpyDeviceToHost));
+    return MB_OK;
+}
+
+int mb_monodomain_device_v(mb_monodomain *m, double **v_dev, void **stream) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    if (v_dev) *v_dev = m->d_v;
+    if (stream) *stream = (void *)m->stream;
+    return MB_OK;
+}
+
+/* Times n steps phase by phase with events on the launching stream: the ODE
+ * kernel alone and the CG solve (initial residual + WHILE loop) alone. */
+int mb_monodomain_profile_steps(mb_monodomain *m, int n, double *ode_ms, double *cg_ms, double *step_ms,
+                                int *cg_iterations) {
+    if (!m || n <= 0) return set_err(MB_ERR_ARG, "bad arguments");
+    double to = 0, tc = 0, ts = 0;
+    long its = 0;
+    for (int i = 0; i < n; ++i) {
+        CK(cudaEventRecord(m->ev[0], m->stream));
+        CKK(mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
+        CK(cudaEventRecord(m->ev[1], m->stream));
+        if (m->use_graphs) {
+            CK(cudaGraphLaunch(m->ge_cg, m->stream));
+        } else {
+            int rc = cg_host_loop(m);
+            if (rc) return rc;
+        }
+        CK(cudaEventRecord(m->ev[2], m->stream));
+        CKK(mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream));
+        CK(cudaEventRecord(m->ev[3], m->stream));
+        CK(cudaEventSynchronize(m->ev[3]));
+        float a = 0, b = 0, c = 0;
+        cudaEventElapsedTime(&a, m->ev[0], m->ev[1]);
+        cudaEventElapsedTime(&b, m->ev[1], m->ev[2]);
+        cudaEventElapsedTime(&c, m->ev[0], m->ev[3]);
+        to += a; tc += b; ts += c;
+        int32_t it = 0;
+        cudaMemcpy(&it, &m->d_ctrl->its, sizeof it, cudaMemcpyDeviceToHost);
+        its += it;
+    }
+    if (ode_ms) *ode_ms = to / n;
+    if (cg_ms) *cg_ms = tc / n;
+    if (step_ms) *step_ms = ts / n;
+    if (cg_iterations) *cg_iterations = (int)(its / n);
+    return MB_OK;
+}
+
+/* ---- general CSR CG -------------------------------------------------------- */
+
+int mb_csr_conjugate_gradient(int32_t n, const int32_t *row_ptr, const int32_t *col, const double *val,
+                              const double *b, double *x, double tolerance, int max_iterations,
+                              int use_preconditioner, uint32_t *number_of_iterations, double *error) {
+    if (n <= 0 || !row_ptr || !col || !val || !b || !x) return set_err(MB_ERR_ARG, "bad arguments");
+    const int32_t nnz = row_ptr[n];
+    mb_csr_dev a;
+    memset(&a, 0, sizeof a);
+    a.n = n;
+    int gb = (n + 255) / 256;
+    if (gb > mbk_max_grid_blocks()) gb = mbk_max_grid_blocks();
+    a.grid_blocks = gb;
+    int32_t *d_rp = NULL, *d_col = NULL;
+    double *d_val = NULL, *d_b = NULL, *d_x = NULL, *d_r = NULL, *d_p = NULL, *d_q = NULL, *d_id = NULL, *d_part = NULL;
+    mb_ctrl *d_ctrl = NULL;
+    cudaStream_t s = NULL;
+    int rc = MB_OK;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CK(cudaMalloc((void **)&d_rp, (size_t)(n + 1) * sizeof(int32_t)));
+    CK(cudaMalloc((void **)&d_col, (size_t)nnz * sizeof(int32_t)));
+    CK(cudaMalloc((void **)&d_val, (size_t)nnz * sizeof(double)));
+    CK(cudaMalloc((void **)&d_b, (size_t)n * sizeof(double)));
+    CK(cudaMalloc((void **)&d_x, (size_t)n * sizeof(double)));
+    CK(cudaMalloc((void **)&d_r, (size_t)n * sizeof(double)));
+    CK(cudaMalloc((void **)&d_p, (size_t)n * sizeof(double)));
+    CK(cudaMalloc((void **)&d_q, (size_t)n * sizeof(double)));
+    CK(cudaMalloc((void **)&d_id, (size_t)n * sizeof(double)));
+    CK(cudaMalloc((void **)&d_part, (size_t)3 * gb * sizeof(double)));
+    CK(cudaMalloc((void **)&d_ctrl, sizeof(mb_ctrl)));
+    CK(cudaMemcpy(d_rp, row_ptr, (size_t)(n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_col, col, (size_t)nnz * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_val, val, (size_t)nnz * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_b, b, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_x, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    mb_ctrl c;
+    memset(&c, 0, sizeof c);
+    c.tol = tolerance;
+    c.max_its = max_iterations;
+    c.use_precond = use_preconditioner ? 1 : 0;
+    CK(cudaMemcpy(d_ctrl, &c, sizeof c, cudaMemcpyHostToDevice));
+    a.row_ptr = d_rp; a.col = d_col; a.val = d_val; a.b = d_b; a.x = d_x; a.r = d_r; a.p = d_p; a.q = d_q;
+    a.inv_diag = d_id; a.partials = d_part;
+    if (mbk_csr_cg_init(&a, d_ctrl, s)) rc = set_err(MB_ERR_CUDA, "csr init launch failed");
+    for (int it = 0; !rc && it < max_iterations + 1; it += 16) {
+        for (int q = 0; q < 16 && !rc; ++q)
+            if (mbk_csr_cg_iter(&a, d_ctrl, s)) rc = set_err(MB_ERR_CUDA, "csr iteration launch failed");
+        int32_t done = 0;
+        cudaMemcpyAsync(&done, &d_ctrl->done, sizeof done, cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        if (done) break;
+    }
+    if (!rc) {
+        cudaMemcpy(&c, d_ctrl, sizeof c, cudaMemcpyDeviceToHost);
+        cudaMemcpy(x, d_x, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+        if (number_of_iterations) *number_of_iterations = (uint32_t)c.its;
+        if (error) *error = c.error;
+    }
+    void *bufs[] = {d_rp, d_col, d_val, d_b, d_x, d_r, d_p, d_q, d_id, d_part, d_ctrl};
+    for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
+    cudaStreamDestroy(s);
+    return rc;
+}

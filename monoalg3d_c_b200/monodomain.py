@@ -1,0 +1,283 @@
+"""Host-side mirror of MonoAlg3D's monodomain plugin interface over the C ABI.
+
+The names follow the reference plugins so that a driver script reads like
+``solve_monodomain`` (src/monodomain/monodomain_solver.c:616-925):
+
+    tissue.solve_all_volumes_odes()        # ode_solver.c:183-248
+    tissue.update_monodomain_default()     # update_monodomain.c:19-56
+    its, err = tissue.conjugate_gradient() # linear_system_solver.c:185-200
+    tissue.advance_time()                  # monodomain_solver.c:907-908
+
+``Tissue.step(n)`` runs n whole loop iterations as captured CUDA graphs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import MbDesc, MbStepStats, MbStim, check, lib
+
+MODELS = {"tt2006": _lib.MB_MODEL_TT2006, "ten_tusscher_2006": _lib.MB_MODEL_TT2006,
+          "torord": _lib.MB_MODEL_TORORD_FKATP_MIXED,
+          "ToRORd_fkatp_mixed_endo_mid_epi": _lib.MB_MODEL_TORORD_FKATP_MIXED}
+PRECISIONS = {"fp64": _lib.MB_PREC_FP64, "mixed": _lib.MB_PREC_MIXED}
+RL_RULES = {"reference_cpu": _lib.MB_RL_REFERENCE_CPU, "true": _lib.MB_RL_TRUE}
+ASSEMBLIES = {"homogeneous": _lib.MB_ASSEMBLY_HOMOGENEOUS, "anisotropic": _lib.MB_ASSEMBLY_ANISOTROPIC,
+              "per_cell": _lib.MB_ASSEMBLY_PER_CELL_SIGMA}
+STIM_KINDS = {"x_less_than": _lib.MB_STIM_X_LESS_THAN, "x_y_limits": _lib.MB_STIM_X_Y_LIMITS,
+              "x_y_z_limits": _lib.MB_STIM_X_Y_Z_LIMITS, "cell_mask": _lib.MB_STIM_CELL_MASK}
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def init_cell_model_data(model: str):
+    """(number_of_ode_equations, initial_v) of a cell model (init_cell_model_data)."""
+    neq, v0 = C.c_int(), C.c_double()
+    check(lib.mb_init_cell_model_data(MODELS[model], C.byref(neq), C.byref(v0)))
+    return neq.value, v0.value
+
+
+def loop_steps(final_time: float, dt: float) -> int:
+    """Iterations of ``while(cur_time - finalT <= dt_pde)`` with ``cur_time += dt_pde``
+    accumulated in double, as the reference loop runs (monodomain_solver.c:616,908)."""
+    cur, n = 0.0, 0
+    while cur - final_time <= dt:
+        n += 1
+        cur += dt
+    return n
+
+
+@dataclass
+class Stim:
+    """One [stim_*] section: stim_if_x_less_than, stim_x_y_limits, stim_x_y_z_limits
+    (stimuli.c:56-91,426-520) or an explicit per-cell mask."""
+    kind: str = "x_less_than"
+    start: float = 0.0
+    duration: float = 2.0
+    current: float = -53.0
+    period: float = 0.0
+    x_limit: float = 500.0
+    min: Sequence[float] = (0.0, 0.0, 0.0)
+    max: Sequence[float] = (0.0, 0.0, 0.0)
+    cell_mask: Optional[np.ndarray] = None
+
+
+class Tissue:
+    """One structured-grid tissue solved on the GPU.
+
+    Arrays given per cell are in grid order (index i + nx*(j + ny*k)).
+    """
+
+    def __init__(self, nx: int, ny: int, nz: int, dx: float = 100.0, dy: float = 100.0, dz: float = 100.0, *,
+                 active: Optional[np.ndarray] = None, dt_pde: float = 0.02, dt_ode: Optional[float] = None,
+                 beta: float = 0.14, cm: float = 1.0, model: str = "tt2006", precision: str = "fp64",
+                 rl_rule: str = "reference_cpu", assembly: str = "homogeneous",
+                 sigma: Sequence[float] = (0.00013, 0.00013, 0.00013), sigma_l: float = 0.0,
+                 sigma_t: float = 0.0, sigma_n: Optional[float] = None,
+                 fibre_angle_z: Optional[np.ndarray] = None, sigma_cell: Optional[np.ndarray] = None,
+                 celltype: Optional[np.ndarray] = None, current_scale: Optional[np.ndarray] = None,
+                 initial_state: Optional[np.ndarray] = None, cg_tolerance: float = 1e-16,
+                 cg_max_iterations: int = 200, use_preconditioner: bool = True,
+                 stims: Sequence[Stim] = (), initial_v: float = float("nan")):
+        self.shape = (nz, ny, nx)
+        self.n = nx * ny * nz
+        d = MbDesc()
+        lib.mb_monodomain_desc_defaults(C.byref(d))
+        d.nx, d.ny, d.nz = nx, ny, nz
+        d.dx, d.dy, d.dz = dx, dy, dz
+        keep = []
+
+        def arr(a, dtype, size=None):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=dtype).reshape(-1)
+            if size is not None and a.size != size:
+                raise ValueError(f"expected {size} values, got {a.size}")
+            keep.append(a)
+            return _ptr(a)
+
+        d.active = arr(active, np.uint8, self.n)
+        d.dt_pde = dt_pde
+        d.dt_ode = dt_pde if dt_ode is None else dt_ode
+        d.beta, d.cm = beta, cm
+        d.model = MODELS[model]
+        d.precision = PRECISIONS[precision]
+        d.rl_rule = RL_RULES[rl_rule]
+        d.initial_state = arr(initial_state, np.float64)
+        d.celltype = arr(celltype, np.uint8, self.n)
+        d.current_scale = arr(current_scale, np.float64, _lib.MB_NUM_SCALES * self.n)
+        d.assembly = ASSEMBLIES[assembly]
+        d.sigma[0], d.sigma[1], d.sigma[2] = sigma
+        d.sigma_l, d.sigma_t = sigma_l, sigma_t
+        d.sigma_n = sigma_t if sigma_n is None else sigma_n
+        d.fibre_angle_z = arr(fibre_angle_z, np.float64, nz)
+        d.sigma_cell = arr(sigma_cell, np.float64, self.n)
+        d.cg_tolerance = cg_tolerance
+        d.cg_max_iterations = cg_max_iterations
+        d.use_preconditioner = 1 if use_preconditioner else 0
+        if len(stims) > _lib.MB_MAX_STIMS:
+            raise ValueError("too many stimuli")
+        d.num_stims = len(stims)
+        for q, s in enumerate(stims):
+            t = d.stims[q]
+            t.kind = STIM_KINDS[s.kind]
+            t.start, t.duration, t.current, t.period = s.start, s.duration, s.current, s.period
+            t.x_limit = s.x_limit
+            for a in range(3):
+                t.min[a] = s.min[a]
+                t.max[a] = s.max[a]
+            t.cell_mask = arr(s.cell_mask, np.uint8, self.n)
+        d.initial_v = initial_v
+        self.model = model
+        self.precision = precision
+        self.active = None if active is None else np.asarray(active, dtype=bool).reshape(-1).copy()
+        h = C.c_void_p()
+        check(lib.mb_monodomain_create(C.byref(h), C.byref(d)))
+        self._h = h
+        del keep
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.mb_monodomain_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- whole steps --------------------------------------------------------
+    def step(self, n: int = 1):
+        check(lib.mb_monodomain_step(self._h, int(n)))
+
+    def sync(self):
+        check(lib.mb_monodomain_sync(self._h))
+
+    def step_host(self, stim: Optional[np.ndarray] = None, v_out: Optional[np.ndarray] = None):
+        """One loop step through host buffers (the reference GPU plugins' copies)."""
+        check(lib.mb_monodomain_step_host(self._h, _ptr(stim), _ptr(v_out)))
+
+    # -- split API, reference names ----------------------------------------
+    def solve_all_volumes_odes(self):
+        check(lib.mb_solve_all_volumes_odes(self._h))
+
+    def update_monodomain_default(self):
+        check(lib.mb_update_monodomain_default(self._h))
+
+    def conjugate_gradient(self):
+        its, err = C.c_uint32(), C.c_double()
+        check(lib.mb_conjugate_gradient(self._h, C.byref(its), C.byref(err)))
+        return its.value, err.value
+
+    def advance_time(self):
+        check(lib.mb_advance_time(self._h))
+
+    # -- state ----------------------------------------------------------------
+    def v(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.float64)
+        check(lib.mb_monodomain_get_v(self._h, _ptr(out)))
+        return out
+
+    def set_v(self, v: np.ndarray):
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+        check(lib.mb_monodomain_set_v(self._h, _ptr(v)))
+
+    def info(self):
+        count, t, na, neq = C.c_int64(), C.c_double(), C.c_uint32(), C.c_int()
+        check(lib.mb_monodomain_info(self._h, C.byref(count), C.byref(t), C.byref(na), C.byref(neq)))
+        return {"count": count.value, "cur_time": t.value, "n_active": na.value, "neq": neq.value}
+
+    def state(self) -> np.ndarray:
+        inf = self.info()
+        out = np.empty((inf["neq"], inf["n_active"]), dtype=np.float64)
+        check(lib.mb_monodomain_get_state(self._h, _ptr(out)))
+        return out
+
+    def step_stats(self, first: int, n: int) -> np.ndarray:
+        buf = (MbStepStats * n)()
+        check(lib.mb_monodomain_step_stats(self._h, first, n, buf))
+        return np.array([(s.cg_iterations, s.refinements, s.cg_error) for s in buf],
+                        dtype=[("its", "i4"), ("refinements", "i4"), ("error", "f8")])
+
+    def device_v(self):
+        p, s = C.c_void_p(), C.c_void_p()
+        check(lib.mb_monodomain_device_v(self._h, C.byref(p), C.byref(s)))
+        return p.value, s.value
+
+    def profile(self, n: int):
+        a, b, c, it = C.c_double(), C.c_double(), C.c_double(), C.c_int()
+        check(lib.mb_monodomain_profile_steps(self._h, n, C.byref(a), C.byref(b), C.byref(c), C.byref(it)))
+        return {"ode_ms": a.value, "cg_ms": b.value, "step_ms": c.value, "cg_iterations": it.value}
+
+
+class OdeSolver:
+    """GPU cell-model library for independent cells (set_model_initial_conditions_gpu /
+    solve_model_odes_gpu, ode_solver.h:37-47)."""
+
+    def __init__(self, model: str, num_cells: int, dt: float, num_steps: int = 1, precision: str = "fp64",
+                 rl_rule: str = "reference_cpu"):
+        h = C.c_void_p()
+        check(lib.mb_ode_create(C.byref(h), MODELS[model], PRECISIONS[precision], RL_RULES[rl_rule],
+                                num_cells, dt, num_steps))
+        self._h = h
+        self.num_cells = num_cells
+        self.neq, self.initial_v = init_cell_model_data(model)
+        self.pitch = None
+
+    def set_model_initial_conditions_gpu(self, initial_state: Optional[np.ndarray] = None,
+                                         celltype: Optional[np.ndarray] = None) -> int:
+        ist = None if initial_state is None else np.ascontiguousarray(initial_state, dtype=np.float64)
+        ct = None if celltype is None else np.ascontiguousarray(celltype, dtype=np.uint8)
+        pitch = C.c_size_t()
+        check(lib.mb_set_model_initial_conditions_gpu(self._h, _ptr(ist), _ptr(ct), C.byref(pitch)))
+        self.pitch = pitch.value
+        return pitch.value
+
+    def solve_model_odes_gpu(self, current_t: float, stim_currents: Optional[np.ndarray] = None):
+        st = None if stim_currents is None else np.ascontiguousarray(stim_currents, dtype=np.float64)
+        check(lib.mb_solve_model_odes_gpu(self._h, current_t, _ptr(st)))
+
+    def state(self) -> np.ndarray:
+        out = np.empty((self.neq, self.num_cells), dtype=np.float64)
+        check(lib.mb_ode_get_state(self._h, _ptr(out)))
+        return out
+
+    def set_state(self, s: np.ndarray):
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        check(lib.mb_ode_set_state(self._h, _ptr(s)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.mb_ode_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def csr_conjugate_gradient(row_ptr, col, val, b, x0=None, tolerance=1e-16, max_iterations=200,
+                           use_preconditioner=True):
+    """Jacobi-PCG on a general CSR matrix (the reference's file-loaded solver test)."""
+    row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    n = b.size
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    its, err = C.c_uint32(), C.c_double()
+    check(lib.mb_csr_conjugate_gradient(n, _ptr(row_ptr), _ptr(col), _ptr(val), _ptr(b), _ptr(x), tolerance,
+                                        max_iterations, 1 if use_preconditioner else 0, C.byref(its),
+                                        C.byref(err)))
+    return x, its.value, err.value
