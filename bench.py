@@ -1,0 +1,314 @@
+"""Benchmark of the operator-split monodomain step (cell-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config 1] [--impl ours|reference]
+
+A step is one iteration of the reference time loop (ODE sub-steps, update_monodomain,
+Jacobi-PCG to r.r <= 1e-16) on the whole tissue.  Default workload: the
+precision configuration, a 200x200x50 slab (2M volumes, 20 % diffuse fibrosis,
+1.6M active) with ToRORd endo cells and fibres along x, run in the
+mixed-precision form; the plain FP64 GPU path is timed beside it and the
+mixed/FP64 ratio and the V difference between the two are reported.
+
+value  -- device time of K captured steps (CUDA events on the launching
+          stream), inputs resident in HBM, max over ranks; whole-job cell-steps/s.
+e2e    -- the same steps through the reference-host C-ABI call
+          (mb_monodomain_step_host): every step copies the stimulus currents
+          host->device and V device->host (pinned host buffers).
+Under torchrun each rank runs an independent replica (the path does not shard:
+one GPU solves one tissue), so scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 4])
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---- distributed plumbing (replicas) -----------------------------------------
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- clocks during the timed region ---------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in self.rows for q in range(4) if len(r) > 5 + q and "Active" in r[5 + q]
+                          and "Not" not in r[5 + q]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_hbm():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---- algorithmic bytes (roofline numerators) --------------------------------------
+
+def cg_bytes(prec: str, n_active: int, n_grid: int, its: float, refinements: float, masked: bool) -> float:
+    """Bytes one CG solve must move at least: per iteration x, r, p each read and
+    written once (Ap and z are not stored); plus the fused right-hand side and
+    initial residual (read V*, read x, write r and p); 1 byte of mask per grid
+    cell per iteration when cells are removed."""
+    mask = n_grid * its if masked else 0.0
+    if prec == "fp64":
+        return n_active * 8.0 * (6 * its + 3) + mask
+    # mixed: x in FP64 (16 B r+w), r and p in FP32 (8 + 8 B); every FP64
+    # residual evaluation reads V* and x (16 B) and writes r, p (8 B)
+    return n_active * (32.0 * its + 24.0 * max(refinements, 1.0)) + mask
+
+
+def ode_bytes(model: str, prec: str, n_active: int) -> float:
+    """State read + written once per cell-step, plus V in and V* out."""
+    per = {("tt2006", "fp64"): 18 * 8, ("tt2006", "mixed"): 5 * 8 + 13 * 4,
+           ("torord", "fp64"): 42 * 8, ("torord", "mixed"): 8 * 8 + 34 * 4}[(model, prec)]
+    return n_active * (2.0 * per + 16.0)
+
+
+# ---- arms -------------------------------------------------------------------------
+
+def run_tissue(wl, prec, steps, warmup, ws):
+    t = wl.tissue(precision=prec)
+    t.step(warmup)
+    t.sync()
+    barrier(ws)
+    ms = t.time_steps(steps)
+    t.sync()
+    ms = allmax(ws, ms)
+    prof = t.profile(3)        # phase times with events: ODE kernel, CG launch
+    stats = t.step_stats(warmup, steps)
+    return t, ms, prof, stats
+
+
+def cpu_baseline(wl, model, assembly):
+    sys.path.insert(0, os.path.join(REPO, "oracle", "ref"))
+    import run_reference
+    if not run_reference.available():
+        return None
+    r = run_reference.run(wl.nx, wl.ny, wl.nz, model, assembly, steps=6,
+                          sigma_l=wl.kwargs.get("sigma_l", 0.0002), sigma_t=wl.kwargs.get("sigma_t", 0.00005))
+    return {"value": r["cell_steps_per_s"], "unit": "cell-steps/s", "cores": r["threads"], "kind": "reference",
+            "sample": f"reference MonoAlg3D CPU path (OpenMP, FP64, Jacobi-PCG 1e-16) on the {wl.nx}x{wl.ny}x{wl.nz} "
+                      f"cuboid without removed cells, {r['steps']} loop steps, Resolution Time - Write Time"}
+
+
+def model_of(wl):
+    return wl.kwargs.get("model", "tt2006")
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args)
+    from monoalg3d_c_b200 import workloads
+    wl = workloads.CONFIGS[args.config](args.scale)
+    model = model_of(wl)
+    assembly = wl.kwargs.get("assembly", "homogeneous")
+    metric = "cell-steps/s (mixed precision)"
+    if args.impl == "reference":
+        if rank == 0:
+            sys.path.insert(0, os.path.join(REPO, "oracle", "ref"))
+            import run_reference
+            if not run_reference.available():
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU build) not built"}))
+                return
+            r = run_reference.run(wl.nx, wl.ny, wl.nz, model, assembly, steps=max(args.steps, 3),
+                                  sigma_l=wl.kwargs.get("sigma_l", 0.0002),
+                                  sigma_t=wl.kwargs.get("sigma_t", 0.00005))
+            v = r["cell_steps_per_s"]
+            sample = (f"reference MonoAlg3D CPU path (OpenMP, FP64) on the {wl.nx}x{wl.ny}x{wl.nz} cuboid without "
+                      f"removed cells, {r['steps']} loop steps")
+            print(json.dumps({
+                "impl": "reference", "metric": metric, "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
+                "steps": r["steps"], "warmup": 0, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": wl.name, "cells": wl.n},
+                "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": r["threads"], "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import ctypes
+    n_active = wl.active_cells()
+    masked = wl.kwargs.get("active") is not None
+    with ClockSampler(local) as clk:
+        t_mx, ms_mx, prof_mx, st_mx = run_tissue(wl, "mixed", args.steps, args.warmup, ws)
+    t_64, ms_64, prof_64, st_64 = run_tissue(wl, "fp64", args.steps, args.warmup, ws)
+
+    # V difference of the two forms after the same steps
+    v_mx, v_64 = t_mx.v(), t_64.v()
+    ok = np.isfinite(v_64)
+    dv = v_mx[ok] - v_64[ok]
+    t_64.close()
+
+    # end to end through the reference-host call with pinned host buffers
+    import torch
+    n_grid = wl.n
+    stim = torch.zeros(n_active, dtype=torch.float64, pin_memory=True)
+    act = wl.kwargs.get("active")
+    cells = np.flatnonzero(act) if act is not None else np.arange(n_grid)
+    x = (cells % wl.nx + 0.5) * 100.0
+    stim.numpy()[:] = np.where(x < 500.0, -53.0, 0.0)
+    vout = torch.empty(n_grid, dtype=torch.float64, pin_memory=True)
+    barrier(ws)
+    ms_e2e = t_mx.time_steps_host(args.steps, ctypes.c_void_p(stim.data_ptr()), ctypes.c_void_p(vout.data_ptr()))
+    ms_e2e = allmax(ws, ms_e2e)
+    tune = t_mx.tuning()
+    t_mx.close()
+
+    cell_steps = n_active * args.steps * ws
+    value = cell_steps / (ms_mx * 1e-3)
+    fp64_value = cell_steps / (ms_64 * 1e-3)
+    e2e = cell_steps / (ms_e2e * 1e-3)
+
+    # roofline of the dominant kernel of the mixed step
+    hbm, hbm_kind = measured_hbm()
+    its = float(np.mean(st_mx["its"]))
+    refs = float(np.mean(st_mx["refinements"]))
+    cg_b = cg_bytes("mixed", n_active, n_grid, its, refs, masked)
+    od_b = ode_bytes(model, "mixed", n_active)
+    if prof_mx["cg_ms"] >= prof_mx["ode_ms"]:
+        name, b, dur = "k_pcg<mixed> (persistent Jacobi-PCG)", cg_b, prof_mx["cg_ms"]
+    else:
+        name, b, dur = f"k_{model}_mixed (Rush-Larsen ODE)", od_b, prof_mx["ode_ms"]
+    achieved = b / (dur * 1e-3) / 1e9
+    roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "traffic": None, "peak_kind": hbm_kind,
+            "bytes_per_launch": b}
+
+    out = {
+        "metric": metric, "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mx / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded Philox fibrosis mask; workload shapes of the precision configuration)",
+        "config": {"workload": wl.name, "cells": n_grid, "active_cells": n_active, "model": model,
+                   "assembly": assembly, "dt_ms": 0.02, "cg_tolerance": 1e-16,
+                   "l2": "inputs larger than L2 (state + vectors > 126 MB per step)",
+                   "parallelism": f"replicas x{ws}"},
+        "fp64": {"value": fp64_value, "ms_per_step": ms_64 / args.steps,
+                 "cg_iterations_per_step": float(np.mean(st_64["its"])),
+                 "ode_ms": prof_64["ode_ms"], "cg_ms": prof_64["cg_ms"]},
+        "mixed_over_fp64": value / fp64_value,
+        "mixed": {"ode_ms": prof_mx["ode_ms"], "cg_ms": prof_mx["cg_ms"], "cg_iterations_per_step": its,
+                  "fp64_residual_evaluations_per_step": refs, "ode_variant": tune["ode_variant"],
+                  "cg_blocks": tune["cg_blocks"], "cg_kernel": tune["cg_kernel"]},
+        "error_vs_fp64": {"v_rms_mv": float(np.sqrt(np.mean(dv ** 2))), "v_max_mv": float(np.max(np.abs(dv))),
+                          "after_steps": args.warmup + args.steps + 3},
+        "roofline": roof,
+        "kernels": {"ode_mixed": {"ms": prof_mx["ode_ms"], "bytes": od_b,
+                                  "GBps": od_b / (prof_mx["ode_ms"] * 1e-3) / 1e9},
+                    "cg_mixed": {"ms": prof_mx["cg_ms"], "bytes": cg_b,
+                                 "GBps": cg_b / (prof_mx["cg_ms"] * 1e-3) / 1e9}},
+        "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": n_active * 8,
+                "d2h_bytes_per_step": n_grid * 8},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_baseline(wl, model, assembly)
+        except Exception as e:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps(out))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -240,6 +240,18 @@ int mb_monodomain_device_v(mb_monodomain *m, double **v_dev, void **stream);
 int mb_monodomain_profile_steps(mb_monodomain *m, int n, double *ode_ms, double *cg_ms,
                                 double *step_ms, int *cg_iterations);
 
+/* Device time (CUDA events on the tissue's stream) of n whole steps, and of n
+ * reference-host steps (mb_monodomain_step_host with the given buffers).    */
+int mb_monodomain_time_steps(mb_monodomain *m, int n, double *ms);
+int mb_monodomain_time_steps_host(mb_monodomain *m, int n, const double *stim_host, double *v_host,
+                                  double *ms);
+
+/* Launch choices made at creation by timing: the ODE kernel's register-budget
+ * variant (0..3 = at least 1..4 resident 128-thread blocks per SM), the CG
+ * grid size and the CG kernel (-1 = graph of separate kernels, 0.. = launch
+ * shape of the persistent kernel, 100 = the 2.5D tiled persistent kernel). */
+int mb_monodomain_tuning(mb_monodomain *m, int *ode_variant, int *cg_blocks, int *cg_kernel);
+
 /* ---- general sparse CG (test_solvers.c fixtures) ---------------------- */
 /* Solves A x = b for a CSR matrix on the device; x holds the initial guess
  * on entry.  Same iteration and stopping rule as cpu_conjugate_gradient

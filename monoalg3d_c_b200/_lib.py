@@ -46,6 +46,7 @@ EXPORTED = [
     "mb_monodomain_step_host", "mb_monodomain_get_v", "mb_monodomain_set_v",
     "mb_monodomain_get_state", "mb_monodomain_info", "mb_monodomain_step_stats",
     "mb_monodomain_device_v", "mb_monodomain_profile_steps", "mb_csr_conjugate_gradient",
+    "mb_monodomain_tuning", "mb_monodomain_time_steps", "mb_monodomain_time_steps_host",
 ]
 
 
@@ -137,6 +138,9 @@ def _load() -> C.CDLL:
         "mb_monodomain_device_v": (i32, [vp, P(vp), P(vp)]),
         "mb_monodomain_profile_steps": (i32, [vp, i32, P(dbl), P(dbl), P(dbl), P(i32)]),
         "mb_csr_conjugate_gradient": (i32, [i32, vp, vp, vp, vp, vp, dbl, i32, i32, P(u32), P(dbl)]),
+        "mb_monodomain_tuning": (i32, [vp, P(i32), P(i32), P(i32)]),
+        "mb_monodomain_time_steps": (i32, [vp, i32, P(dbl)]),
+        "mb_monodomain_time_steps_host": (i32, [vp, i32, vp, vp, P(dbl)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -83,7 +83,15 @@ typedef struct mb_ode_dev {
     const float   *scale;     /* MB_NUM_SCALES rows of ld, NULL = 1         */
     const double  *stim_host; /* per compact cell external stimulus, or NULL */
     double dt;
+    int32_t variant;          /* register-budget variant chosen by the autotuner */
+    uint32_t out_ld;          /* row stride of out64/out32                  */
+    double *out64;            /* if set, the new state goes here (tuning)   */
+    float  *out32;
 } mb_ode_dev;
+
+#define MB_ODE_VARIANTS 4     /* min resident blocks of 128 threads: 1, 2, 3, 4 */
+int mbk_ode_step_mixed(const mb_ode_dev *o, mb_ctrl *ctrl, const double *vin, double *vout,
+                       cudaStream_t s);
 
 /* ---- kernel launchers (kernels.cu) ------------------------------------ */
 int mbk_ode_init(const mb_ode_dev *o, const double *table_dev, int ntypes, cudaStream_t s);
@@ -126,6 +134,36 @@ int mbk_csr_cg_init(const mb_csr_dev *a, mb_ctrl *ctrl, cudaStream_t s);
 int mbk_csr_cg_iter(const mb_csr_dev *a, mb_ctrl *ctrl, cudaStream_t s);
 
 int mbk_max_grid_blocks(void);
+
+/* Persistent cooperative CG (one launch per solve). */
+typedef struct mb_pcg_dev {
+    mb_stencil_dev st;
+    int mixed;
+    int blocks;
+    double *x;
+    const double *vstar;
+    const double *b;
+    double *r64, *pa64, *pb64;
+    float *r32, *pa32, *pb32;
+    double *z64;             /* preconditioned residual (flat kernel)     */
+    float *z32;
+    const double *inv_diag64;/* Jacobi 1/diag (FP64 form)   */
+    const float *inv_diag32; /* Jacobi 1/diag (mixed form)  */
+    double *partials;        /* 2 * 4 * blocks */
+    mb_ctrl *ctrl;
+    unsigned *bar;           /* 2 words, zero at start */
+    int *status;             /* 0 = ok; set on a barrier timeout */
+    int tiled;               /* 1 = 2.5D tiled passes (cg_tiled.cu) */
+    int variant;             /* launch-shape variant of cg_flat.cu */
+    int tiles_x, tiles_y, zchunk, nchunks;
+} mb_pcg_dev;
+int mbk_fcg_variants(int kind);
+int mbk_fcg_max_blocks(int mixed, int kind, int variant);
+int mbk_fcg_launch(const mb_pcg_dev *p, cudaStream_t s);
+int mbk_tcg_max_blocks(int mixed);
+int mbk_tcg_launch(const mb_pcg_dev *p, cudaStream_t s);
+void mbk_tcg_layout(int nx, int ny, int nz, int blocks, int *tiles_x, int *tiles_y, int *zchunk, int *nchunks);
+int mbk_inv_diag(const mb_stencil_dev *st, double *d64, float *d32, cudaStream_t s);
 
 #ifdef __cplusplus
 }

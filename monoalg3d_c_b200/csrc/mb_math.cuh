@@ -5,7 +5,16 @@
 #pragma once
 #include <cuda_runtime.h>
 
-namespace mb {
+// Device code compiled with and without MB_FAST_FP32_MATH lives in different
+// inline namespaces, so the two translation units never share a definition.
+#ifdef MB_FAST_FP32_MATH
+#define MB_NS_BEGIN namespace mb { inline namespace fastf {
+#else
+#define MB_NS_BEGIN namespace mb { inline namespace accf {
+#endif
+#define MB_NS_END } }
+
+MB_NS_BEGIN
 
 __device__ __forceinline__ double mexp(double x) { return exp(x); }
 __device__ __forceinline__ double mlog(double x) { return log(x); }
@@ -16,12 +25,13 @@ __device__ __forceinline__ double mpow(double x, double y) { return pow(x, y); }
 #ifdef MB_FAST_FP32_MATH
 __device__ __forceinline__ float mexp(float x) { return __expf(x); }
 __device__ __forceinline__ float mlog(float x) { return __logf(x); }
+__device__ __forceinline__ float mpow(float x, float y) { return __powf(x, y); }
 #else
+__device__ __forceinline__ float mpow(float x, float y) { return powf(x, y); }
 __device__ __forceinline__ float mexp(float x) { return expf(x); }
 __device__ __forceinline__ float mlog(float x) { return logf(x); }
 #endif
 __device__ __forceinline__ float msqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ float mexpm1(float x) { return expm1f(x); }
-__device__ __forceinline__ float mpow(float x, float y) { return powf(x, y); }
 
-}  // namespace mb
+MB_NS_END

@@ -20,7 +20,7 @@
 #pragma once
 #include "mb_math.cuh"
 
-namespace mb {
+MB_NS_BEGIN
 
 constexpr int TOR_NEQ = 43;
 constexpr int TOR_N64 = 9;    // mixed form: V and the 8 ion concentrations in FP64
@@ -587,4 +587,4 @@ __host__ __device__ inline double torord_default_state(int celltype, int s) {
     return endo[s];
 }
 
-}  // namespace mb
+MB_NS_END

@@ -14,7 +14,7 @@
 #pragma once
 #include "mb_math.cuh"
 
-namespace mb {
+MB_NS_BEGIN
 
 constexpr int TT_NEQ = 19;
 
@@ -238,4 +238,4 @@ __device__ __forceinline__ void tt2006_rhs(const T *y, T stim, T dt, const TTSca
     u.gate[11] = r_inf + (r - r_inf) * mexp(-dt / tau_r);
 }
 
-}  // namespace mb
+MB_NS_END

@@ -253,6 +253,14 @@ struct mb_monodomain {
     mb_step_stats *d_log;
     int64_t log_len;
     uint8_t *h_mask;      /* owned copy of desc.active (NULL = all active) */
+    /* persistent CG */
+    int use_pcg;
+    mb_pcg_dev pcg;
+    double *d_pb, *d_ppart, *d_invd, *d_z;
+    float *d_pb32, *d_invd32, *d_z32;
+    unsigned *d_bar;
+    int *d_status;
+    float cg_tune_ms;     /* device time of one CG solve of the chosen kernel at tuning */
 
     mb_ode_dev ode;
     mb_stencil_dev st;
@@ -304,7 +312,8 @@ void mb_monodomain_destroy(mb_monodomain *m) {
     if (!m) return;
     if (m->stream) cudaStreamSynchronize(m->stream);
     destroy_graphs(m);
-    void *bufs[] = {m->d_mask, m->d_cells, m->d_v, m->d_vstar, m->d_r, m->d_p, m->d_r32, m->d_p32,
+    void *bufs[] = {m->d_pb, m->d_ppart, m->d_pb32, m->d_bar, m->d_status, m->d_invd, m->d_invd32, m->d_z, m->d_z32,
+                    m->d_mask, m->d_cells, m->d_v, m->d_vstar, m->d_r, m->d_p, m->d_r32, m->d_p32,
                     m->d_partials, m->d_sv64, m->d_sv32, m->d_stim_bits, m->d_celltype, m->d_scale,
                     m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_stim_host, m->d_ctrl, m->d_log};
     for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
@@ -349,6 +358,80 @@ static int stim_covers(const mb_stim *s, const double c[3], int64_t g) {
     } while (0)
 
 static int build_graphs(mb_monodomain *m);
+static int ode_autotune(mb_monodomain *m);
+
+/* Picks the CG kernel: every launch-shape variant of the flat persistent
+ * kernel and the 2.5D tiled one solve the tissue's first system (b = alpha V*
+ * from the initial state) twice; V is restored after every trial and the
+ * fastest by CUDA events is kept.  MB_CG_VARIANT=<n> (n = number of flat
+ * variants selects the tiled kernel) forces a choice. */
+static int cg_autotune(mb_monodomain *m) {
+    if (!m->use_pcg) return MB_OK;
+    const int mixed = m->pcg.mixed;
+    const int kind = m->st.kind;
+    const int nv = mbk_fcg_variants(kind);
+    const char *env = getenv("MB_CG_VARIANT");
+    int lo = 0, hi = nv;          /* candidates 0..nv-1 flat, nv tiled */
+    if (env) lo = hi = atoi(env);
+    double *vsave = NULL;
+    if (cudaMalloc((void **)&vsave, (size_t)m->n * sizeof(double)) != cudaSuccess)
+        return set_err(MB_ERR_NOMEM, "CG tuning buffer");
+    cudaMemcpyAsync(vsave, m->d_v, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+    float best = 1e30f;
+    int bestc = lo, rc = MB_OK;
+    for (int cand = lo; cand <= hi && !rc; ++cand) {
+        mb_pcg_dev q = m->pcg;
+        if (cand < nv) {
+            q.tiled = 0;
+            q.variant = cand;
+            q.blocks = mbk_fcg_max_blocks(mixed, kind, cand);
+        } else {
+            q.tiled = 1;
+            const int items = q.tiles_x * q.tiles_y * q.nchunks;
+            const int mb = mbk_tcg_max_blocks(mixed);
+            q.blocks = items < mb ? items : mb;
+        }
+        if (q.blocks <= 0) continue;
+        float tsum = 0;
+        for (int rep = 0; rep < 3 && !rc; ++rep) {
+            cudaMemcpyAsync(m->d_v, vsave, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+            cudaEventRecord(m->ev[0], m->stream);
+            const int e = q.tiled ? mbk_tcg_launch(&q, m->stream) : mbk_fcg_launch(&q, m->stream);
+            cudaEventRecord(m->ev[1], m->stream);
+            if (e || cudaEventSynchronize(m->ev[1]) != cudaSuccess) {
+                rc = set_err(MB_ERR_CUDA, "CG tuning launch failed (candidate %d): %s", cand,
+                             cudaGetErrorString(e ? (cudaError_t)e : cudaGetLastError()));
+                break;
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, m->ev[0], m->ev[1]);
+            if (rep > 0) tsum += ms;      /* first run warms up */
+        }
+        if (!rc && tsum < best) {
+            best = tsum;
+            bestc = cand;
+        }
+    }
+    cudaMemcpyAsync(m->d_v, vsave, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+    cudaStreamSynchronize(m->stream);
+    cudaFree(vsave);
+    if (rc) return rc;
+    int st = 0;
+    cudaMemcpy(&st, m->d_status, sizeof st, cudaMemcpyDeviceToHost);
+    if (st) return set_err(MB_ERR_CUDA, "CG grid barrier timed out during tuning");
+    if (bestc < nv) {
+        m->pcg.tiled = 0;
+        m->pcg.variant = bestc;
+        m->pcg.blocks = mbk_fcg_max_blocks(mixed, kind, bestc);
+    } else {
+        m->pcg.tiled = 1;
+        const int items = m->pcg.tiles_x * m->pcg.tiles_y * m->pcg.nchunks;
+        const int mb = mbk_tcg_max_blocks(mixed);
+        m->pcg.blocks = items < mb ? items : mb;
+    }
+    m->cg_tune_ms = best / 2.0f;
+    return MB_OK;
+}
 
 int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
     int rc = MB_OK;
@@ -498,6 +581,9 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         if (e) { rc = set_err(MB_ERR_CUDA, "V* init failed"); goto fail; }
     }
 
+    rc = ode_autotune(m);
+    if (rc) goto fail;
+
     /* diffusion operator */
     m->st.nx = d->nx; m->st.ny = d->ny; m->st.nz = d->nz;
     m->st.alpha = mb_alpha(d->beta, d->cm, d->dt_pde, d->dx, d->dy, d->dz);
@@ -553,6 +639,71 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
     m->cg.r32 = m->d_r32; m->cg.p32 = m->d_p32;
     m->cg.partials = m->d_partials;
 
+    /* persistent cooperative CG: one launch per solve */
+    {
+        const char *mode = getenv("MB_CG");
+        m->use_pcg = !(mode && strcmp(mode, "graph") == 0);
+        const int mixed = d->precision == MB_PREC_MIXED;
+        int maxb = -1;
+        if (m->use_pcg) {
+            /* the partials buffer must fit the largest grid of any variant */
+            const int nv = mbk_fcg_variants(m->st.kind);
+            for (int v = 0; v < nv; ++v) {
+                const int b = mbk_fcg_max_blocks(mixed, m->st.kind, v);
+                if (b > maxb) maxb = b;
+            }
+            const int bt = mbk_tcg_max_blocks(mixed);
+            if (bt > maxb) maxb = bt;
+            mbk_tcg_layout(d->nx, d->ny, d->nz, bt > 0 ? bt : 1, &m->pcg.tiles_x, &m->pcg.tiles_y, &m->pcg.zchunk,
+                           &m->pcg.nchunks);
+        }
+        if (maxb <= 0) m->use_pcg = 0;
+        if (m->use_pcg) {
+            const int blocks = maxb;
+            if (d->precision == MB_PREC_FP64) {
+                ALLOC(m->d_pb, (size_t)n * sizeof(double));
+                CKK(cudaMemset(m->d_pb, 0, (size_t)n * sizeof(double)));
+                ALLOC(m->d_z, (size_t)n * sizeof(double));
+                CKK(cudaMemset(m->d_z, 0, (size_t)n * sizeof(double)));
+            } else {
+                ALLOC(m->d_pb32, (size_t)n * sizeof(float));
+                CKK(cudaMemset(m->d_pb32, 0, (size_t)n * sizeof(float)));
+                ALLOC(m->d_z32, (size_t)n * sizeof(float));
+                CKK(cudaMemset(m->d_z32, 0, (size_t)n * sizeof(float)));
+            }
+            ALLOC(m->d_ppart, ((size_t)8 * blocks + 8) * sizeof(double));
+            if (d->precision == MB_PREC_FP64) {
+                ALLOC(m->d_invd, (size_t)n * sizeof(double));
+                CKK(cudaMemset(m->d_invd, 0, (size_t)n * sizeof(double)));
+            } else {
+                ALLOC(m->d_invd32, (size_t)n * sizeof(float));
+                CKK(cudaMemset(m->d_invd32, 0, (size_t)n * sizeof(float)));
+            }
+            CKK(mbk_inv_diag(&m->st, m->d_invd, m->d_invd32, m->stream));
+            CKK(cudaStreamSynchronize(m->stream));
+            ALLOC(m->d_bar, 2 * sizeof(unsigned));
+            ALLOC(m->d_status, sizeof(int));
+            CKK(cudaMemset(m->d_bar, 0, 2 * sizeof(unsigned)));
+            CKK(cudaMemset(m->d_status, 0, sizeof(int)));
+            mb_pcg_dev *q = &m->pcg;
+            q->mixed = d->precision == MB_PREC_MIXED;
+            q->tiled = 0;
+            q->variant = 0;
+            q->blocks = mbk_fcg_max_blocks(mixed, m->st.kind, 0);
+            q->x = m->d_v;
+            q->vstar = m->d_vstar;
+            q->b = NULL;
+            q->r64 = m->d_r; q->pa64 = m->d_p; q->pb64 = m->d_pb;
+            q->r32 = m->d_r32; q->pa32 = m->d_p32; q->pb32 = m->d_pb32;
+            q->z64 = m->d_z; q->z32 = m->d_z32;
+            q->partials = m->d_ppart;
+            q->inv_diag64 = m->d_invd;
+            q->inv_diag32 = m->d_invd32;
+            q->bar = m->d_bar;
+            q->status = m->d_status;
+        }
+    }
+
     /* control block */
     {
         mb_ctrl c;
@@ -572,10 +723,14 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         c.refine_ratio = 1e-8;
         ALLOC(m->d_ctrl, sizeof(mb_ctrl));
         UPLOAD(m->d_ctrl, &c, sizeof c);
+        m->pcg.ctrl = m->d_ctrl;
+        m->pcg.st = m->st;
     }
     m->log_len = 1 << 20;
     ALLOC(m->d_log, (size_t)m->log_len * sizeof(mb_step_stats));
 
+    rc = cg_autotune(m);
+    if (rc) goto fail;
     rc = build_graphs(m);
     if (rc) goto fail;
 
@@ -601,6 +756,61 @@ fail:
     mb_assembly_free(&asmb);
     mb_monodomain_destroy(m);
     return rc ? rc : MB_ERR_CUDA;
+}
+
+/* Picks the register-budget variant of the ODE kernel: each variant advances
+ * up to 2^20 cells from the current state into scratch buffers (the live
+ * state is not touched) and the fastest by CUDA events wins. */
+static int ode_autotune(mb_monodomain *m) {
+    const char *env = getenv("MB_ODE_VARIANT");
+    if (env) {
+        m->ode.variant = atoi(env);
+        return MB_OK;
+    }
+    int n64, n32;
+    ode_rows(m->desc.model, m->desc.precision, &n64, &n32);
+    const uint32_t nt = m->n_active < (1u << 20) ? m->n_active : (1u << 20);
+    double *s64 = NULL, *vs = NULL;
+    float *s32 = NULL;
+    int rc = MB_OK;
+    if (cudaMalloc((void **)&s64, (size_t)n64 * nt * sizeof(double)) != cudaSuccess ||
+        (n32 && cudaMalloc((void **)&s32, (size_t)n32 * nt * sizeof(float)) != cudaSuccess) ||
+        cudaMalloc((void **)&vs, (size_t)m->n * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(s64); cudaFree(s32); cudaFree(vs);
+        m->ode.variant = 0;
+        return MB_OK;           /* no room to tune: keep the default */
+    }
+    mb_ode_dev t = m->ode;
+    t.n = nt;
+    t.stim_bits = NULL;
+    t.out64 = s64;
+    t.out32 = s32;
+    t.out_ld = nt;
+    float best = 1e30f;
+    int bestv = 0;
+    for (int v = 0; v < MB_ODE_VARIANTS && !rc; ++v) {
+        t.variant = v;
+        if (mbk_ode_step(&t, NULL, m->d_vstar, vs, m->stream)) { rc = set_err(MB_ERR_CUDA, "ODE tuning launch failed"); break; }
+        cudaEventRecord(m->ev[0], m->stream);
+        for (int q = 0; q < 3; ++q) mbk_ode_step(&t, NULL, m->d_vstar, vs, m->stream);
+        cudaEventRecord(m->ev[1], m->stream);
+        if (cudaEventSynchronize(m->ev[1]) != cudaSuccess) { rc = set_err(MB_ERR_CUDA, "ODE tuning failed"); break; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, m->ev[0], m->ev[1]);
+        if (ms < best) { best = ms; bestv = v; }
+    }
+    cudaFree(s64); cudaFree(s32); cudaFree(vs);
+    m->ode.variant = bestv;
+    return rc;
+}
+
+int mb_monodomain_tuning(mb_monodomain *m, int *ode_variant, int *cg_blocks, int *cg_kernel) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    if (ode_variant) *ode_variant = m->ode.variant;
+    if (cg_blocks) *cg_blocks = m->use_pcg ? m->pcg.blocks : m->cg.grid_blocks;
+    if (cg_kernel) *cg_kernel = !m->use_pcg ? -1 : (m->pcg.tiled ? 100 : m->pcg.variant);
+    return MB_OK;
 }
 
 /* Captures the launches of fn into a fresh graph. */
@@ -681,10 +891,24 @@ static int build_loop_graph(mb_monodomain *m, capture_fn pre, capture_fn post, c
     return MB_OK;
 }
 
+static int cap_pcg_step(mb_monodomain *m, int in_body) {
+    (void)in_body;
+    int e = mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream);
+    if (!e) e = m->pcg.tiled ? mbk_tcg_launch(&m->pcg, m->stream) : mbk_fcg_launch(&m->pcg, m->stream);
+    if (!e) e = mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream);
+    return e;
+}
+
 static int build_graphs(mb_monodomain *m) {
     if (!m->use_graphs) return MB_OK;
-    int rc = build_loop_graph(m, cap_pre, cap_post, &m->g_step, &m->ge_step);
-    if (!rc) rc = build_loop_graph(m, cap_cginit, NULL, &m->g_cg, &m->ge_cg);
+    int rc;
+    if (m->use_pcg) {
+        rc = capture_graph(m, cap_pcg_step, &m->g_step);
+        if (!rc) CK(cudaGraphInstantiate(&m->ge_step, m->g_step, 0));
+    } else {
+        rc = build_loop_graph(m, cap_pre, cap_post, &m->g_step, &m->ge_step);
+        if (!rc) rc = build_loop_graph(m, cap_cginit, NULL, &m->g_cg, &m->ge_cg);
+    }
     if (rc) {
         /* fall back to host-driven launches */
         cudaGetLastError();
@@ -712,13 +936,26 @@ static int cg_host_loop(mb_monodomain *m) {
     return MB_OK;
 }
 
+/* Enqueues one CG solve (initial residual from V*, then iterations). */
+static int cg_enqueue(mb_monodomain *m) {
+    if (m->use_pcg) {
+        CKK(m->pcg.tiled ? mbk_tcg_launch(&m->pcg, m->stream) : mbk_fcg_launch(&m->pcg, m->stream));
+        return MB_OK;
+    }
+    if (m->use_graphs) {
+        CK(cudaGraphLaunch(m->ge_cg, m->stream));
+        return MB_OK;
+    }
+    return cg_host_loop(m);
+}
+
 static int step_once(mb_monodomain *m) {
     if (m->use_graphs) {
         CK(cudaGraphLaunch(m->ge_step, m->stream));
         return MB_OK;
     }
     CKK(mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
-    int rc = cg_host_loop(m);
+    int rc = cg_enqueue(m);
     if (rc) return rc;
     CKK(mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream));
     return MB_OK;
@@ -739,6 +976,11 @@ int mb_monodomain_sync(mb_monodomain *m) {
     CK(cudaStreamSynchronize(m->stream));
     int32_t nan_flag = 0;
     CK(cudaMemcpy(&nan_flag, &m->d_ctrl->nan_flag, sizeof nan_flag, cudaMemcpyDeviceToHost));
+    if (m->d_status) {
+        int st = 0;
+        CK(cudaMemcpy(&st, m->d_status, sizeof st, cudaMemcpyDeviceToHost));
+        if (st) return set_err(MB_ERR_CUDA, "CG grid barrier timed out (status %d)", st);
+    }
     if (nan_flag) return set_err(MB_ERR_NAN, "NaN in the CG error: the cell model diverged");
     return MB_OK;
 }
@@ -765,10 +1007,8 @@ int mb_update_monodomain_default(mb_monodomain *m) {
 int mb_conjugate_gradient(mb_monodomain *m, uint32_t *its, double *error) {
     if (!m) return set_err(MB_ERR_ARG, "null");
     if (m->phase != 2) return set_err(MB_ERR_STATE, "conjugate_gradient before update_monodomain");
-    if (m->use_graphs) {
-        CK(cudaGraphLaunch(m->ge_cg, m->stream));
-    } else {
-        int rc = cg_host_loop(m);
+    {
+        int rc = cg_enqueue(m);
         if (rc) return rc;
     }
     mb_ctrl c;
@@ -797,10 +1037,8 @@ int mb_monodomain_step_host(mb_monodomain *m, const double *stim_host, double *v
         o.stim_host = m->d_stim_host;
     }
     CKK(mbk_ode_step(&o, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
-    if (m->use_graphs) {
-        CK(cudaGraphLaunch(m->ge_cg, m->stream));
-    } else {
-        int rc = cg_host_loop(m);
+    {
+        int rc = cg_enqueue(m);
         if (rc) return rc;
     }
     CKK(mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream));
@@ -870,6 +1108,36 @@ int mb_monodomain_device_v(mb_monodomain *m, double **v_dev, void **stream) {
 
 /* Times n steps phase by phase with events on the launching stream: the ODE
  * kernel alone and the CG solve (initial residual + WHILE loop) alone. */
+/* Device time of n whole steps, CUDA events on the tissue's stream. */
+int mb_monodomain_time_steps(mb_monodomain *m, int n, double *ms) {
+    if (!m || n <= 0 || !ms) return set_err(MB_ERR_ARG, "bad arguments");
+    CK(cudaEventRecord(m->ev[0], m->stream));
+    int rc = mb_monodomain_step(m, n);
+    if (rc) return rc;
+    CK(cudaEventRecord(m->ev[1], m->stream));
+    CK(cudaEventSynchronize(m->ev[1]));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, m->ev[0], m->ev[1]));
+    *ms = t;
+    return MB_OK;
+}
+
+/* Device time of n reference-host steps (stimulus H2D, ODE, CG, V D2H). */
+int mb_monodomain_time_steps_host(mb_monodomain *m, int n, const double *stim_host, double *v_host, double *ms) {
+    if (!m || n <= 0 || !ms) return set_err(MB_ERR_ARG, "bad arguments");
+    CK(cudaEventRecord(m->ev[2], m->stream));
+    for (int i = 0; i < n; ++i) {
+        int rc = mb_monodomain_step_host(m, stim_host, v_host);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(m->ev[3], m->stream));
+    CK(cudaEventSynchronize(m->ev[3]));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, m->ev[2], m->ev[3]));
+    *ms = t;
+    return MB_OK;
+}
+
 int mb_monodomain_profile_steps(mb_monodomain *m, int n, double *ode_ms, double *cg_ms, double *step_ms,
                                 int *cg_iterations) {
     if (!m || n <= 0) return set_err(MB_ERR_ARG, "bad arguments");
@@ -879,10 +1147,8 @@ int mb_monodomain_profile_steps(mb_monodomain *m, int n, double *ode_ms, double 
         CK(cudaEventRecord(m->ev[0], m->stream));
         CKK(mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
         CK(cudaEventRecord(m->ev[1], m->stream));
-        if (m->use_graphs) {
-            CK(cudaGraphLaunch(m->ge_cg, m->stream));
-        } else {
-            int rc = cg_host_loop(m);
+        {
+            int rc = cg_enqueue(m);
             if (rc) return rc;
         }
         CK(cudaEventRecord(m->ev[2], m->stream));

@@ -1,0 +1,227 @@
+// Per-cell ionic ODE kernels: one thread per cell, state in structure-of-arrays
+// rows so that every row load/store of a warp is one coalesced transaction;
+// all num_steps sub-steps run with the state in registers.  MINB is the
+// minimum number of resident 128-thread blocks per SM the register allocation
+// must allow (the autotuner picks one per model and precision).
+//
+// Reference behaviour followed:
+//   sub-step loop per cell        ten_tusscher_2006_RS_CPU.c:74-98,
+//                                 ToRORd_fkatp_mixed_endo_mid_epi.c:165-250
+//   stimulus merge per sub-step   ode_solver.c:201-235 (window inclusive)
+//   V taken from the grid only when cur_time > 0
+//                                 monodomain_solver.c:660-661
+#pragma once
+#include <cstdint>
+#include "mb_internal.h"
+#include "model_tt2006.cuh"
+#include "model_torord.cuh"
+
+MB_NS_BEGIN
+
+constexpr int ODE_THREADS = 128;
+
+// Merged stimulus of compact cell t for the current loop step: every stimulus
+// config whose bit is set adds its current once per sub-step whose time lies
+// in [start, start + duration] (ode_solver.c:213-222).
+__device__ __forceinline__ double cell_stim(const mb_ode_dev &o, const mb_ctrl *__restrict__ c, uint32_t t) {
+    if (o.stim_host) return o.stim_host[t];
+    if (!o.stim_bits) return 0.0;
+    const unsigned bits = o.stim_bits[t];
+    if (!bits) return 0.0;
+    double s = 0.0;
+    const int ns = c->num_stims;
+    for (int k = 0; k < ns; ++k) {
+        if (!((bits >> k) & 1u)) continue;
+        const double start = c->stim_start[k];
+        const double end = start + c->stim_dur[k];
+        const double cur = c->stim_current[k];
+        double time = c->cur_time;
+        for (int j = 0; j < o.num_steps; ++j) {
+            if (time >= start && time <= end) s += cur;
+            time += o.dt;
+        }
+    }
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ TTScale<T> load_tt_scale(const mb_ode_dev &o, uint32_t t) {
+    TTScale<T> sc;
+    if (o.scale) {
+        sc.gNa = T(o.scale[0 * (size_t)o.ld + t]);
+        sc.gKr = T(o.scale[1 * (size_t)o.ld + t]);
+        sc.gKs = T(o.scale[2 * (size_t)o.ld + t]);
+        sc.gCaL = T(o.scale[3 * (size_t)o.ld + t]);
+        sc.gK1 = T(o.scale[4 * (size_t)o.ld + t]);
+    } else {
+        sc.gNa = sc.gKr = sc.gKs = sc.gCaL = sc.gK1 = T(1);
+    }
+    return sc;
+}
+
+// Where the new state goes: in place, or into the tuning buffers.
+__device__ __forceinline__ double *out64(const mb_ode_dev &o) { return o.out64 ? o.out64 : o.sv64; }
+__device__ __forceinline__ float *out32(const mb_ode_dev &o) { return o.out64 ? o.out32 : o.sv32; }
+__device__ __forceinline__ size_t out_ld(const mb_ode_dev &o) { return o.out64 ? o.out_ld : o.ld; }
+
+// ---- ten Tusscher 2006 ----------------------------------------------------
+// FP64 layout: sv64 row s = state s (row 0 unused when V lives in the grid).
+// Mixed layout: sv64 rows {V, Ca_i, Ca_SR, Ca_ss, Na_i, K_i};
+//               sv32 rows {Xr1 .. r (12 gates), R'}.
+template <int MINB>
+__global__ void __launch_bounds__(ODE_THREADS, MINB)
+k_tt2006_fp64(mb_ode_dev o, const mb_ctrl *__restrict__ ctrl, const double *__restrict__ vin,
+              double *__restrict__ vout) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= o.n) return;
+    const uint32_t g = o.cell ? o.cell[t] : t;
+    const double stim = cell_stim(o, ctrl, t);
+    const size_t ld = o.ld;
+    const double *src = (ctrl == nullptr || ctrl->cur_time > 0.0) ? vin : vout;
+    double y[TT_NEQ];
+    y[0] = src[g];
+#pragma unroll
+    for (int s = 1; s < TT_NEQ; ++s) y[s] = o.sv64[s * ld + t];
+    const TTScale<double> sc = load_tt_scale<double>(o, t);
+    const double dt = o.dt;
+    for (int step = 0; step < o.num_steps; ++step) {
+        TTUpdate<double> u;
+        tt2006_rhs<double>(y, stim, dt, sc, u);
+        y[TT_V] = dt * u.dV + y[TT_V];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) y[1 + k] = u.gate[k];
+        y[TT_CAI] = dt * u.dCai + y[TT_CAI];
+        y[TT_CASR] = dt * u.dCaSR + y[TT_CASR];
+        y[TT_CASS] = dt * u.dCaSS + y[TT_CASS];
+        y[TT_RPRIME] = dt * u.dRprime + y[TT_RPRIME];
+        y[TT_NAI] = dt * u.dNai + y[TT_NAI];
+        y[TT_KI] = dt * u.dKi + y[TT_KI];
+    }
+    vout[g] = y[0];
+    double *w = out64(o);
+    const size_t wl = out_ld(o);
+#pragma unroll
+    for (int s = 1; s < TT_NEQ; ++s) w[s * wl + t] = y[s];
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(ODE_THREADS, MINB)
+k_tt2006_mixed(mb_ode_dev o, const mb_ctrl *__restrict__ ctrl, const double *__restrict__ vin,
+               double *__restrict__ vout) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= o.n) return;
+    const uint32_t g = o.cell ? o.cell[t] : t;
+    const float stim = (float)cell_stim(o, ctrl, t);
+    const size_t ld = o.ld;
+    const double *src = (ctrl == nullptr || ctrl->cur_time > 0.0) ? vin : vout;
+    double V = src[g];
+    double cai = o.sv64[1 * ld + t], casr = o.sv64[2 * ld + t], cass = o.sv64[3 * ld + t];
+    double nai = o.sv64[4 * ld + t], ki = o.sv64[5 * ld + t];
+    float gates[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) gates[k] = o.sv32[k * ld + t];
+    float rprime = o.sv32[12 * ld + t];
+    const TTScale<float> sc = load_tt_scale<float>(o, t);
+    const double dt = o.dt;
+    const float dtf = (float)dt;
+    for (int step = 0; step < o.num_steps; ++step) {
+        float y[TT_NEQ];
+        y[TT_V] = (float)V;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) y[1 + k] = gates[k];
+        y[TT_CAI] = (float)cai; y[TT_CASR] = (float)casr; y[TT_CASS] = (float)cass;
+        y[TT_RPRIME] = rprime; y[TT_NAI] = (float)nai; y[TT_KI] = (float)ki;
+        TTUpdate<float> u;
+        tt2006_rhs<float>(y, stim, dtf, sc, u);
+        V = dt * (double)u.dV + V;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) gates[k] = u.gate[k];
+        cai = dt * (double)u.dCai + cai;
+        casr = dt * (double)u.dCaSR + casr;
+        cass = dt * (double)u.dCaSS + cass;
+        rprime = dtf * u.dRprime + rprime;
+        nai = dt * (double)u.dNai + nai;
+        ki = dt * (double)u.dKi + ki;
+    }
+    vout[g] = V;
+    double *w = out64(o);
+    float *w32 = out32(o);
+    const size_t wl = out_ld(o);
+    w[1 * wl + t] = cai; w[2 * wl + t] = casr; w[3 * wl + t] = cass;
+    w[4 * wl + t] = nai; w[5 * wl + t] = ki;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) w32[k * wl + t] = gates[k];
+    w32[12 * wl + t] = rprime;
+}
+
+// ---- ToRORd-fkatp endo/mid/epi -------------------------------------------
+// FP64 layout: sv64 row s = state s.
+// Mixed layout: sv64 rows {V, cass, nai, nass, ki, kss, cansr, cajsr, cai},
+//               sv32 rows {CaMKt, states 10..42}.
+template <int RULE, int MINB>
+__global__ void __launch_bounds__(ODE_THREADS, MINB)
+k_torord_fp64(mb_ode_dev o, const mb_ctrl *__restrict__ ctrl, const double *__restrict__ vin,
+              double *__restrict__ vout) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= o.n) return;
+    const uint32_t g = o.cell ? o.cell[t] : t;
+    const double stim = cell_stim(o, ctrl, t);
+    const size_t ld = o.ld;
+    const double *src = (ctrl == nullptr || ctrl->cur_time > 0.0) ? vin : vout;
+    double y[TOR_NEQ];
+    y[0] = src[g];
+#pragma unroll
+    for (int s = 1; s < TOR_NEQ; ++s) y[s] = o.sv64[s * ld + t];
+    const double celltype = o.celltype ? (double)o.celltype[t] : 0.0;
+    TorScale<double> sc;
+    load_tor_scale(o.scale, ld, t, sc);
+    const double dt = o.dt;
+    for (int step = 0; step < o.num_steps; ++step) torord_rl_step<double, double, RULE>(y, stim, dt, celltype, sc);
+    vout[g] = y[0];
+    double *w = out64(o);
+    const size_t wl = out_ld(o);
+#pragma unroll
+    for (int s = 1; s < TOR_NEQ; ++s) w[s * wl + t] = y[s];
+}
+
+template <int RULE, int MINB>
+__global__ void __launch_bounds__(ODE_THREADS, MINB)
+k_torord_mixed(mb_ode_dev o, const mb_ctrl *__restrict__ ctrl, const double *__restrict__ vin,
+               double *__restrict__ vout) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= o.n) return;
+    const uint32_t g = o.cell ? o.cell[t] : t;
+    const double stim = cell_stim(o, ctrl, t);
+    const size_t ld = o.ld;
+    const double *src = (ctrl == nullptr || ctrl->cur_time > 0.0) ? vin : vout;
+    TorMixedState st;
+    st.d[0] = src[g];
+#pragma unroll
+    for (int r = 1; r < TOR_N64; ++r) st.d[r] = o.sv64[r * ld + t];
+#pragma unroll
+    for (int r = 0; r < TOR_N32; ++r) st.f[r] = o.sv32[r * ld + t];
+    const float celltype = o.celltype ? (float)o.celltype[t] : 0.0f;
+    TorScale<float> sc;
+    load_tor_scale(o.scale, ld, t, sc);
+    const double dt = o.dt;
+    for (int step = 0; step < o.num_steps; ++step) torord_mixed_step<RULE>(st, stim, dt, celltype, sc);
+    vout[g] = st.d[0];
+    double *w = out64(o);
+    float *w32 = out32(o);
+    const size_t wl = out_ld(o);
+#pragma unroll
+    for (int r = 1; r < TOR_N64; ++r) w[r * wl + t] = st.d[r];
+#pragma unroll
+    for (int r = 0; r < TOR_N32; ++r) w32[r * wl + t] = st.f[r];
+}
+
+// Launch of one (model, precision) family with the variant's register budget.
+#define MB_VARIANT_SWITCH(variant, LAUNCH) \
+    switch (variant) {                     \
+    case 0: LAUNCH(1); break;              \
+    case 1: LAUNCH(2); break;              \
+    case 2: LAUNCH(3); break;              \
+    default: LAUNCH(4); break;             \
+    }
+
+MB_NS_END

@@ -216,6 +216,23 @@ class Tissue:
         check(lib.mb_monodomain_device_v(self._h, C.byref(p), C.byref(s)))
         return p.value, s.value
 
+    def time_steps(self, n: int) -> float:
+        """Device milliseconds of n whole steps (CUDA events on the tissue's stream)."""
+        ms = C.c_double()
+        check(lib.mb_monodomain_time_steps(self._h, int(n), C.byref(ms)))
+        return ms.value
+
+    def time_steps_host(self, n: int, stim_ptr, v_ptr) -> float:
+        """Device milliseconds of n steps through host buffers (raw pointers, e.g. pinned memory)."""
+        ms = C.c_double()
+        check(lib.mb_monodomain_time_steps_host(self._h, int(n), stim_ptr, v_ptr, C.byref(ms)))
+        return ms.value
+
+    def tuning(self):
+        v, b, pc = C.c_int(), C.c_int(), C.c_int()
+        check(lib.mb_monodomain_tuning(self._h, C.byref(v), C.byref(b), C.byref(pc)))
+        return {"ode_variant": v.value, "cg_blocks": b.value, "cg_kernel": pc.value}
+
     def profile(self, n: int):
         a, b, c, it = C.c_double(), C.c_double(), C.c_double(), C.c_int()
         check(lib.mb_monodomain_profile_steps(self._h, n, C.byref(a), C.byref(b), C.byref(c), C.byref(it)))
