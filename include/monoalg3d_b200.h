@@ -261,6 +261,27 @@ int mb_csr_conjugate_gradient(int32_t n, const int32_t *row_ptr, const int32_t *
                               double tolerance, int max_iterations, int use_preconditioner,
                               uint32_t *number_of_iterations, double *error);
 
+/* ---- allocation-free CSR CG -------------------------------------------- */
+/* No counterpart in the reference.  The same solve as
+ * mb_csr_conjugate_gradient for callers that cannot allocate device memory
+ * while they run (a host framework that owns all device memory through its
+ * own pool, a real-time loop that cannot afford cudaMalloc's synchronisation,
+ * a plugin handed device buffers by its host): row_ptr, col, val, b and x are
+ * DEVICE pointers supplied by the caller, x holds the initial guess and
+ * receives the solution, and the work vectors live in a fixed 16 MiB + 64 KiB
+ * device array inside this library (held on every GPU that loads it until
+ * exit).  Nothing is allocated or freed.  n is limited to 524288 rows;
+ * larger systems are rejected with MB_ERR_ARG.  The array's device address is
+ * looked up on the first call made while a device is current: make that
+ * first call before any stream capture on the device.  All calls share the
+ * array, so calls whose work overlaps on the GPU race and must be serialised
+ * by the caller.  stream may be NULL (legacy default stream).  Returns the
+ * iteration count and the final r.r in host memory.                          */
+int mb_csr_conjugate_gradient_noalloc(int32_t n, const int32_t *row_ptr, const int32_t *col,
+                                      const double *val, const double *b, double *x,
+                                      double tolerance, int max_iterations, int use_preconditioner,
+                                      uint32_t *number_of_iterations, double *error, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,6 +47,7 @@ EXPORTED = [
     "mb_monodomain_get_state", "mb_monodomain_info", "mb_monodomain_step_stats",
     "mb_monodomain_device_v", "mb_monodomain_profile_steps", "mb_csr_conjugate_gradient",
     "mb_monodomain_tuning", "mb_monodomain_time_steps", "mb_monodomain_time_steps_host",
+    "mb_csr_conjugate_gradient_noalloc",
 ]
 
 
@@ -141,6 +142,7 @@ def _load() -> C.CDLL:
         "mb_monodomain_tuning": (i32, [vp, P(i32), P(i32), P(i32)]),
         "mb_monodomain_time_steps": (i32, [vp, i32, P(dbl)]),
         "mb_monodomain_time_steps_host": (i32, [vp, i32, vp, vp, P(dbl)]),
+        "mb_csr_conjugate_gradient_noalloc": (i32, [i32, vp, vp, vp, vp, vp, dbl, i32, i32, P(u32), P(dbl), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

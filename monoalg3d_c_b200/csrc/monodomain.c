@@ -33,6 +33,9 @@ static int set_err(int code, const char *fmt, ...) {
 }
 
 const char *mb_last_error(void) { return g_err; }
+
+/* Error reporting for the allocation-free entry point (csr_noalloc.cu). */
+int mb_noalloc_set_error(int code, const char *msg) { return set_err(code, "%s", msg); }
 int mb_version(void) { return 10000; }
 
 #define CK(call)                                                                           \
