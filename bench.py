@@ -39,8 +39,8 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--config", type=int, default=1, choices=[0, 1, 4])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -82,7 +82,9 @@ def allmax(ws, x: float) -> float:
 # ---- clocks during the timed region ---------------------------------------------
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms while the
+    timed steps run (the sampler is started just before and stopped just
+    after them)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -96,7 +98,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -104,13 +106,18 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def wait_first(self, limit_s: float = 3.0):
+        t0 = time.time()
+        while self.proc and not self.rows and time.time() - t0 < limit_s:
+            time.sleep(0.01)
+        self.rows.clear()
+
     def _read(self):
         for line in self.proc.stdout:
             self.rows.append([c.strip() for c in line.split(",")])
 
     def __exit__(self, *exc):
         if self.proc:
-            time.sleep(0.25)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -162,17 +169,19 @@ def ode_bytes(model: str, prec: str, n_active: int) -> float:
 
 # ---- arms -------------------------------------------------------------------------
 
-def run_tissue(wl, prec, steps, warmup, ws):
+def run_tissue(wl, prec, steps, warmup, ws, gpu):
     t = wl.tissue(precision=prec)
     t.step(warmup)
     t.sync()
     barrier(ws)
-    ms = t.time_steps(steps)
+    with ClockSampler(gpu) as clk:
+        clk.wait_first()           # sampler running before the first timed step
+        ms = t.time_steps(steps)
     t.sync()
     ms = allmax(ws, ms)
     prof = t.profile(3)        # phase times with events: ODE kernel, CG launch
     stats = t.step_stats(warmup, steps)
-    return t, ms, prof, stats
+    return t, ms, prof, stats, clk.summary()
 
 
 def cpu_baseline(wl, model, assembly):
@@ -225,9 +234,8 @@ def main():
     import ctypes
     n_active = wl.active_cells()
     masked = wl.kwargs.get("active") is not None
-    with ClockSampler(local) as clk:
-        t_mx, ms_mx, prof_mx, st_mx = run_tissue(wl, "mixed", args.steps, args.warmup, ws)
-    t_64, ms_64, prof_64, st_64 = run_tissue(wl, "fp64", args.steps, args.warmup, ws)
+    t_mx, ms_mx, prof_mx, st_mx, clk_mx = run_tissue(wl, "mixed", args.steps, args.warmup, ws, local)
+    t_64, ms_64, prof_64, st_64, clk_64 = run_tissue(wl, "fp64", args.steps, args.warmup, ws, local)
 
     # V difference of the two forms after the same steps
     v_mx, v_64 = t_mx.v(), t_64.v()
@@ -281,7 +289,7 @@ def main():
                    "parallelism": f"replicas x{ws}"},
         "fp64": {"value": fp64_value, "ms_per_step": ms_64 / args.steps,
                  "cg_iterations_per_step": float(np.mean(st_64["its"])),
-                 "ode_ms": prof_64["ode_ms"], "cg_ms": prof_64["cg_ms"]},
+                 "ode_ms": prof_64["ode_ms"], "cg_ms": prof_64["cg_ms"], "clocks": clk_64},
         "mixed_over_fp64": value / fp64_value,
         "mixed": {"ode_ms": prof_mx["ode_ms"], "cg_ms": prof_mx["cg_ms"], "cg_iterations_per_step": its,
                   "fp64_residual_evaluations_per_step": refs, "ode_variant": tune["ode_variant"],
@@ -296,7 +304,7 @@ def main():
         "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": n_active * 8,
                 "d2h_bytes_per_step": n_grid * 8},
         "gpu_launches": 3 * args.steps,
-        "clocks": clk.summary(),
+        "clocks": clk_mx,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
