@@ -15,7 +15,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 from dataclasses import dataclass, field
-from typing import Optional, Sequence
+from typing import Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -69,6 +69,71 @@ class Stim:
     cell_mask: Optional[np.ndarray] = None
 
 
+def build_desc(nx: int, ny: int, nz: int, dx: float = 100.0, dy: float = 100.0, dz: float = 100.0, *,
+               active: Optional[np.ndarray] = None, dt_pde: float = 0.02, dt_ode: Optional[float] = None,
+               beta: float = 0.14, cm: float = 1.0, model: str = "tt2006", precision: str = "fp64",
+               rl_rule: str = "reference_cpu", assembly: str = "homogeneous",
+               sigma: Sequence[float] = (0.00013, 0.00013, 0.00013), sigma_l: float = 0.0,
+               sigma_t: float = 0.0, sigma_n: Optional[float] = None,
+               fibre_angle_z: Optional[np.ndarray] = None, sigma_cell: Optional[np.ndarray] = None,
+               celltype: Optional[np.ndarray] = None, current_scale: Optional[np.ndarray] = None,
+               initial_state: Optional[np.ndarray] = None, cg_tolerance: float = 1e-16,
+               cg_max_iterations: int = 200, use_preconditioner: bool = True,
+               stims: Sequence[Stim] = (), initial_v: float = float("nan")) -> Tuple[MbDesc, list]:
+    """The C-ABI tissue description (mb_monodomain_desc) for these arguments,
+    with the arrays it points to (keep them alive while the description is
+    in use).  Arrays given per cell are in grid order."""
+    n = nx * ny * nz
+    d = MbDesc()
+    lib.mb_monodomain_desc_defaults(C.byref(d))
+    d.nx, d.ny, d.nz = nx, ny, nz
+    d.dx, d.dy, d.dz = dx, dy, dz
+    keep = []
+
+    def arr(a, dtype, size=None):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=dtype).reshape(-1)
+        if size is not None and a.size != size:
+            raise ValueError(f"expected {size} values, got {a.size}")
+        keep.append(a)
+        return _ptr(a)
+
+    d.active = arr(active, np.uint8, n)
+    d.dt_pde = dt_pde
+    d.dt_ode = dt_pde if dt_ode is None else dt_ode
+    d.beta, d.cm = beta, cm
+    d.model = MODELS[model]
+    d.precision = PRECISIONS[precision]
+    d.rl_rule = RL_RULES[rl_rule]
+    d.initial_state = arr(initial_state, np.float64)
+    d.celltype = arr(celltype, np.uint8, n)
+    d.current_scale = arr(current_scale, np.float64, _lib.MB_NUM_SCALES * n)
+    d.assembly = ASSEMBLIES[assembly]
+    d.sigma[0], d.sigma[1], d.sigma[2] = sigma
+    d.sigma_l, d.sigma_t = sigma_l, sigma_t
+    d.sigma_n = sigma_t if sigma_n is None else sigma_n
+    d.fibre_angle_z = arr(fibre_angle_z, np.float64, nz)
+    d.sigma_cell = arr(sigma_cell, np.float64, n)
+    d.cg_tolerance = cg_tolerance
+    d.cg_max_iterations = cg_max_iterations
+    d.use_preconditioner = 1 if use_preconditioner else 0
+    if len(stims) > _lib.MB_MAX_STIMS:
+        raise ValueError("too many stimuli")
+    d.num_stims = len(stims)
+    for q, s in enumerate(stims):
+        t = d.stims[q]
+        t.kind = STIM_KINDS[s.kind]
+        t.start, t.duration, t.current, t.period = s.start, s.duration, s.current, s.period
+        t.x_limit = s.x_limit
+        for a in range(3):
+            t.min[a] = s.min[a]
+            t.max[a] = s.max[a]
+        t.cell_mask = arr(s.cell_mask, np.uint8, n)
+    d.initial_v = initial_v
+    return d, keep
+
+
 class Tissue:
     """One structured-grid tissue solved on the GPU.
 
@@ -88,53 +153,13 @@ class Tissue:
                  stims: Sequence[Stim] = (), initial_v: float = float("nan")):
         self.shape = (nz, ny, nx)
         self.n = nx * ny * nz
-        d = MbDesc()
-        lib.mb_monodomain_desc_defaults(C.byref(d))
-        d.nx, d.ny, d.nz = nx, ny, nz
-        d.dx, d.dy, d.dz = dx, dy, dz
-        keep = []
-
-        def arr(a, dtype, size=None):
-            if a is None:
-                return None
-            a = np.ascontiguousarray(a, dtype=dtype).reshape(-1)
-            if size is not None and a.size != size:
-                raise ValueError(f"expected {size} values, got {a.size}")
-            keep.append(a)
-            return _ptr(a)
-
-        d.active = arr(active, np.uint8, self.n)
-        d.dt_pde = dt_pde
-        d.dt_ode = dt_pde if dt_ode is None else dt_ode
-        d.beta, d.cm = beta, cm
-        d.model = MODELS[model]
-        d.precision = PRECISIONS[precision]
-        d.rl_rule = RL_RULES[rl_rule]
-        d.initial_state = arr(initial_state, np.float64)
-        d.celltype = arr(celltype, np.uint8, self.n)
-        d.current_scale = arr(current_scale, np.float64, _lib.MB_NUM_SCALES * self.n)
-        d.assembly = ASSEMBLIES[assembly]
-        d.sigma[0], d.sigma[1], d.sigma[2] = sigma
-        d.sigma_l, d.sigma_t = sigma_l, sigma_t
-        d.sigma_n = sigma_t if sigma_n is None else sigma_n
-        d.fibre_angle_z = arr(fibre_angle_z, np.float64, nz)
-        d.sigma_cell = arr(sigma_cell, np.float64, self.n)
-        d.cg_tolerance = cg_tolerance
-        d.cg_max_iterations = cg_max_iterations
-        d.use_preconditioner = 1 if use_preconditioner else 0
-        if len(stims) > _lib.MB_MAX_STIMS:
-            raise ValueError("too many stimuli")
-        d.num_stims = len(stims)
-        for q, s in enumerate(stims):
-            t = d.stims[q]
-            t.kind = STIM_KINDS[s.kind]
-            t.start, t.duration, t.current, t.period = s.start, s.duration, s.current, s.period
-            t.x_limit = s.x_limit
-            for a in range(3):
-                t.min[a] = s.min[a]
-                t.max[a] = s.max[a]
-            t.cell_mask = arr(s.cell_mask, np.uint8, self.n)
-        d.initial_v = initial_v
+        d, keep = build_desc(nx, ny, nz, dx, dy, dz, active=active, dt_pde=dt_pde, dt_ode=dt_ode, beta=beta,
+                             cm=cm, model=model, precision=precision, rl_rule=rl_rule, assembly=assembly,
+                             sigma=sigma, sigma_l=sigma_l, sigma_t=sigma_t, sigma_n=sigma_n,
+                             fibre_angle_z=fibre_angle_z, sigma_cell=sigma_cell, celltype=celltype,
+                             current_scale=current_scale, initial_state=initial_state,
+                             cg_tolerance=cg_tolerance, cg_max_iterations=cg_max_iterations,
+                             use_preconditioner=use_preconditioner, stims=stims, initial_v=initial_v)
         self.model = model
         self.precision = precision
         self.active = None if active is None else np.asarray(active, dtype=bool).reshape(-1).copy()

@@ -1,0 +1,165 @@
+"""ctypes front end of the CPU oracle (oracle/_build/liboracle.so) -- TEST
+INFRASTRUCTURE ONLY.
+
+Used by the tests, the smoke check and bench.py's CPU-baseline leg to check
+and time against; the product never imports it.  The tissue arguments are
+the product's (monoalg3d_c_b200.monodomain.build_desc), so a test hands the
+same description to the GPU tissue and to the oracle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads the oracle library, building it with make if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    lib = C.CDLL(LIB_PATH)
+    vp, i32, u32p, dp = C.c_void_p, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_double)
+    lib.orc_create.argtypes = [C.POINTER(vp), vp]
+    lib.orc_step.argtypes = [vp, C.c_int]
+    lib.orc_get_v.argtypes = [vp, vp]
+    lib.orc_get_state.argtypes = [vp, C.c_int, vp]
+    lib.orc_last_cg.argtypes = [vp, u32p, dp]
+    lib.orc_time.argtypes = [vp]
+    lib.orc_time.restype = C.c_double
+    lib.orc_active_cells.argtypes = [vp]
+    lib.orc_active_cells.restype = i32
+    lib.orc_destroy.argtypes = [vp]
+    lib.orc_loop_steps.argtypes = [C.c_double, C.c_double]
+    lib.orc_tt2006_initial_state.argtypes = [vp]
+    lib.orc_tt2006_step.argtypes = [vp, C.c_double, C.c_double, vp]
+    lib.orc_torord_initial_state.argtypes = [C.c_int, vp]
+    lib.orc_torord_step.argtypes = [vp, C.c_double, C.c_double, C.c_int, C.c_int, vp]
+    lib.orc_assemble.argtypes = [vp, vp, vp]
+    lib.orc_csr_free.argtypes = [vp]
+    lib.orc_pcg.argtypes = [vp, vp, vp, C.c_double, C.c_int, C.c_int, u32p, dp]
+    _lib = lib
+    return lib
+
+
+class Csr(C.Structure):
+    _fields_ = [("n", C.c_int32), ("row_ptr", C.POINTER(C.c_int32)), ("col", C.POINTER(C.c_int32)),
+                ("val", C.POINTER(C.c_double))]
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _desc(nx, ny, nz, **kw):
+    from monoalg3d_c_b200.monodomain import build_desc
+    return build_desc(nx, ny, nz, **kw)
+
+
+class Sim:
+    """The reference time loop on the CPU for a tissue described with the
+    product's arguments (precision is ignored: the oracle is FP64)."""
+
+    def __init__(self, nx: int, ny: int, nz: int, **kw):
+        lib = load()
+        kw = dict(kw)
+        kw.pop("precision", None)
+        self.n = nx * ny * nz
+        d, keep = _desc(nx, ny, nz, **kw)
+        self._keep = (d, keep)            # arrays the description points to
+        h = C.c_void_p()
+        rc = lib.orc_create(C.byref(h), C.byref(d))
+        if rc != 0:
+            raise RuntimeError(f"orc_create failed ({rc})")
+        self._h = h
+        self.model = kw.get("model", "tt2006")
+
+    def step(self, n: int = 1) -> int:
+        return load().orc_step(self._h, int(n))
+
+    def v(self) -> np.ndarray:
+        out = np.empty(self.n)
+        load().orc_get_v(self._h, _p(out))
+        return out
+
+    def state(self, var: int) -> np.ndarray:
+        out = np.empty(load().orc_active_cells(self._h))
+        load().orc_get_state(self._h, int(var), _p(out))
+        return out
+
+    def last_cg(self):
+        its, err = C.c_uint32(), C.c_double()
+        load().orc_last_cg(self._h, C.byref(its), C.byref(err))
+        return its.value, err.value
+
+    @property
+    def time(self) -> float:
+        return load().orc_time(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def assemble(nx: int, ny: int, nz: int, **kw):
+    """(row_ptr, col, val, cells) of the tissue's matrix alpha I + K over the
+    active cells in grid order; cells = grid index of each row."""
+    lib = load()
+    d, keep = _desc(nx, ny, nz, **kw)
+    A = Csr()
+    cells = np.empty(nx * ny * nz, dtype=np.int32)
+    rc = lib.orc_assemble(C.byref(d), C.byref(A), _p(cells))
+    if rc != 0:
+        raise RuntimeError(f"orc_assemble failed ({rc})")
+    n = A.n
+    rp = np.ctypeslib.as_array(A.row_ptr, shape=(n + 1,)).copy()
+    nnz = int(rp[-1])
+    col = np.ctypeslib.as_array(A.col, shape=(max(nnz, 1),))[:nnz].copy()
+    val = np.ctypeslib.as_array(A.val, shape=(max(nnz, 1),))[:nnz].copy()
+    lib.orc_csr_free(C.byref(A))
+    return rp, col, val, cells[:n].copy()
+
+
+def pcg(row_ptr, col, val, b, x0, tol=1e-16, max_its=200, use_preconditioner=True):
+    """cpu_conjugate_gradient on a CSR matrix (diagonal first in each row)."""
+    lib = load()
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    cl = np.ascontiguousarray(col, dtype=np.int32)
+    vl = np.ascontiguousarray(val, dtype=np.float64)
+    A = Csr(int(rp.size - 1), rp.ctypes.data_as(C.POINTER(C.c_int32)), cl.ctypes.data_as(C.POINTER(C.c_int32)),
+            vl.ctypes.data_as(C.POINTER(C.c_double)))
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.array(x0, dtype=np.float64, copy=True)
+    its, err = C.c_uint32(), C.c_double()
+    lib.orc_pcg(C.byref(A), _p(bb), _p(x), tol, int(max_its), 1 if use_preconditioner else 0, C.byref(its),
+                C.byref(err))
+    return x, its.value, err.value
+
+
+def tt2006_initial_state() -> np.ndarray:
+    out = np.empty(19)
+    load().orc_tt2006_initial_state(_p(out))
+    return out
+
+
+def torord_initial_state(celltype: int = 0) -> np.ndarray:
+    out = np.empty(43)
+    load().orc_torord_initial_state(int(celltype), _p(out))
+    return out
+
+
+def loop_steps(final_time: float, dt: float) -> int:
+    return load().orc_loop_steps(final_time, dt)
