@@ -143,7 +143,8 @@ typedef struct mb_monodomain_desc {
                                           1 mid, 2 epi; NULL = all endo       */
     const double *current_scale;       /* per-cell conductance scalings,
                                           MB_NUM_SCALES x (nx*ny*nz), row
-                                          major by scale; NULL = all 1        */
+                                          major by scale; NULL = all 1; kept
+                                          and applied as float values         */
     /* [assembly_matrix] */
     int    assembly;                   /* enum mb_assembly                    */
     double sigma[3];                   /* homogeneous: sigma_x, sigma_y, sigma_z (mS/um) */
@@ -162,6 +163,11 @@ typedef struct mb_monodomain_desc {
        (set_initial_conditions_fvm, matrix_assembly.c:27-45);
        NaN = the model's INITIAL_V                                          */
     double initial_v;
+    /* activation time / APD90 per active cell, tracked on the device (see
+       mb_monodomain_get_activation); 0 = off                               */
+    int    track_activation;
+    double activation_threshold;       /* mV, default -30                     */
+    double activation_min_interval;    /* ms, default 10                      */
 } mb_monodomain_desc;
 
 /* Scalings of the ionic conductances, in this order (TT2006: gNa, gKr, gKs,
@@ -233,6 +239,29 @@ int mb_monodomain_get_state(mb_monodomain *m, double *state_host);  /* NEQ x n_a
 int mb_monodomain_info(mb_monodomain *m, int64_t *count, double *cur_time,
                        uint32_t *n_active, int *neq);
 int mb_monodomain_step_stats(mb_monodomain *m, int64_t first, int64_t n, mb_step_stats *out);
+/* Activation times per grid cell, tracked on the device at every loop step
+ * (needs track_activation): an activation is an upward crossing of
+ * activation_threshold at least activation_min_interval after the previous
+ * one (the rules of save_with_activation_times, save_mesh.c:754-913), its
+ * time linearly interpolated between the two loop steps; APD90 runs from it
+ * to the downward crossing of V_peak - 0.9 (V_peak - V_rest), also
+ * interpolated.  first / last: first and latest activation time (ms),
+ * apd90: APD90 of the latest beat (ms), count: activations.  Cells never
+ * activated, beats not yet repolarised and removed cells read -1 (count 0).
+ * Any pointer may be NULL.                                                  */
+int mb_monodomain_get_activation(mb_monodomain *m, float *first, float *last, float *apd90, int32_t *count);
+
+/* ---- batches of independent tissues ------------------------------------
+ * No counterpart in the reference (which runs one tissue per process).  The
+ * n tissues, tissue i a 2-D sheet nx[i] x ny[i] (ny[i] = 1: a cable), are
+ * placed side by side in one 2-D atlas grid with removed cells between them,
+ * so that no face couples two tissues; the atlas is then solved as one
+ * tissue (one ODE launch, one persistent CG launch and one graph replay per
+ * step for the whole batch), with per-tissue parameters given as per-cell
+ * arrays.  Tissue i occupies atlas cells (x0[i] + i', y0[i] + j') for
+ * 0 <= i' < nx[i], 0 <= j' < ny[i].  Shelf packing, tallest first.          */
+int mb_batch_pack(int n, const int *nx, const int *ny, int *atlas_nx, int *atlas_ny, int *x0, int *y0);
+
 /* Device pointers to V (double, grid order) and to the CUDA stream used. */
 int mb_monodomain_device_v(mb_monodomain *m, double **v_dev, void **stream);
 /* Average duration of the last kernel launches per kind, from CUDA events

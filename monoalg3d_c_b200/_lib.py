@@ -43,7 +43,8 @@ EXPORTED = [
     "mb_monodomain_desc_defaults", "mb_monodomain_create", "mb_monodomain_destroy",
     "mb_monodomain_step", "mb_monodomain_sync", "mb_solve_all_volumes_odes",
     "mb_update_monodomain_default", "mb_conjugate_gradient", "mb_advance_time",
-    "mb_monodomain_step_host", "mb_monodomain_get_v", "mb_monodomain_set_v",
+    "mb_monodomain_step_host", "mb_monodomain_get_v", "mb_monodomain_set_v", "mb_monodomain_get_activation",
+    "mb_batch_pack",
     "mb_monodomain_get_state", "mb_monodomain_info", "mb_monodomain_step_stats",
     "mb_monodomain_device_v", "mb_monodomain_profile_steps", "mb_csr_conjugate_gradient",
     "mb_monodomain_tuning", "mb_monodomain_time_steps", "mb_monodomain_time_steps_host",
@@ -87,6 +88,9 @@ class MbDesc(C.Structure):
         ("num_stims", C.c_int),
         ("stims", MbStim * MB_MAX_STIMS),
         ("initial_v", C.c_double),
+        ("track_activation", C.c_int),
+        ("activation_threshold", C.c_double),
+        ("activation_min_interval", C.c_double),
     ]
 
 
@@ -132,6 +136,8 @@ def _load() -> C.CDLL:
         "mb_advance_time": (i32, [vp]),
         "mb_monodomain_step_host": (i32, [vp, vp, vp]),
         "mb_monodomain_get_v": (i32, [vp, vp]),
+        "mb_monodomain_get_activation": (i32, [vp, vp, vp, vp, vp]),
+        "mb_batch_pack": (i32, [i32, vp, vp, P(i32), P(i32), vp, vp]),
         "mb_monodomain_set_v": (i32, [vp, vp]),
         "mb_monodomain_get_state": (i32, [vp, vp]),
         "mb_monodomain_info": (i32, [vp, P(i64), P(dbl), P(u32), P(i32)]),

@@ -1,4 +1,4 @@
-// Persistent Jacobi-PCG with 2.5D tiling: the same solve as cg_persistent.cu
+// Persistent Jacobi-PCG with 2.5D tiling: the same solve as cg_flat.cu
 // (recurrences and stopping rule of cpu_conjugate_gradient,
 // linear_system_solver.c:47-183; b = alpha V* fused, update_monodomain.c:41-52)
 // but every pass streams the grid as tiles of 30 x 14 cells marching in z.
@@ -11,8 +11,8 @@
 // 27-point row from the planes k-1, k, k+1.  Each field value is loaded from
 // global memory once per tile (plus the halo), instead of once per neighbour
 // use.  Work items are (tile, z-chunk) pairs handed to the persistent blocks in
-// a fixed order; the grid reductions and the bounded barrier are the ones of
-// cg_persistent.cu.
+// a fixed order; the grid reductions use a bounded barrier (the last block
+// to arrive adds the partials and publishes a new generation).
 #include <cstdint>
 #include <type_traits>
 #include <cuda/atomic>
@@ -43,9 +43,8 @@ struct Args {
     int tiles_x, tiles_y, zchunk, nchunks;
 };
 
-// Grid-wide sum (same protocol as cg_persistent.cu: fixed-order sum of block
-// partials by the last block to arrive, release/acquire generation word,
-// bounded wait).
+// Grid-wide sum: fixed-order sum of block partials by the last block to
+// arrive, release/acquire generation word, bounded wait.
 template <int NV>
 __device__ __forceinline__ bool grid_reduce(const Args &a, double (&v)[NV], double (&out)[NV], int &red) {
     __shared__ double sm[NV][THREADS / 32];
@@ -437,6 +436,9 @@ extern "C" int mbk_tcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
     a.inv_diag64 = p->inv_diag64; a.inv_diag32 = p->inv_diag32;
     a.partials = p->partials; a.ctrl = p->ctrl; a.bar = p->bar; a.status = p->status;
     a.tiles_x = p->tiles_x; a.tiles_y = p->tiles_y; a.zchunk = p->zchunk; a.nchunks = p->nchunks;
+    // the barrier words start from zero in every launch
+    cudaError_t e = cudaMemsetAsync(p->bar, 0, 2 * sizeof(unsigned), s);
+    if (e != cudaSuccess) return (int)e;
     void *args[] = {&a};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(p->blocks);

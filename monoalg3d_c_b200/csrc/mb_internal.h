@@ -46,6 +46,10 @@ typedef struct mb_ctrl {
     int32_t use_precond;
     uint32_t ticket;
     uint32_t pad_;
+    /* activation tracking (ODE kernels) */
+    double  act_dt;          /* loop step dt_pde                            */
+    float   act_threshold;   /* upward crossing that marks an activation    */
+    float   act_min_interval;/* ms between two counted activations          */
 } mb_ctrl;
 
 /* Structured grid, device view. */
@@ -67,6 +71,10 @@ typedef struct mb_stencil_dev {
     const double  *fx, *fy, *fz;
     const double  *table;     /* kind 2: [nz][9][27]                        */
     const float   *table32;   /* kind 2, FP32 copy                          */
+    const uint8_t *code;      /* kinds 0, 1: per cell, bit q (q = 0..5 for
+                                 -x,+x,-y,+y,-z,+z) = that neighbour couples,
+                                 bit 6 = the cell is active                 */
+    const uint16_t *rowid;    /* kind 2: per cell, k * 9 + class            */
 } mb_stencil_dev;
 
 /* ODE state, device view.  Rows of double (sv64) and float (sv32), each of
@@ -87,7 +95,19 @@ typedef struct mb_ode_dev {
     uint32_t out_ld;          /* row stride of out64/out32                  */
     double *out64;            /* if set, the new state goes here (tuning)   */
     float  *out32;
+    float  *act;              /* activation tracking, MB_ACT_ROWS rows of ld,
+                                 NULL = off                                 */
 } mb_ode_dev;
+
+/* Rows of the activation-tracking array (per compact cell). */
+#define MB_ACT_VPREV 0        /* V at the previous loop step (NaN = none)   */
+#define MB_ACT_FIRST 1        /* first activation time, ms (-1 = none)      */
+#define MB_ACT_LAST 2         /* latest activation time, ms (-1 = none)     */
+#define MB_ACT_APD 3          /* APD90 of the latest beat, ms (-1 = open)   */
+#define MB_ACT_VPEAK 4        /* peak V since the latest activation         */
+#define MB_ACT_VREST 5        /* lowest V since the last repolarisation     */
+#define MB_ACT_STATE 6        /* 2 x activations + (1 while depolarised)    */
+#define MB_ACT_ROWS 7
 
 #define MB_ODE_VARIANTS 4     /* min resident blocks of 128 threads: 1, 2, 3, 4 */
 int mbk_ode_step_mixed(const mb_ode_dev *o, mb_ctrl *ctrl, const double *vin, double *vout,
@@ -164,6 +184,7 @@ int mbk_tcg_max_blocks(int mixed);
 int mbk_tcg_launch(const mb_pcg_dev *p, cudaStream_t s);
 void mbk_tcg_layout(int nx, int ny, int nz, int blocks, int *tiles_x, int *tiles_y, int *zchunk, int *nchunks);
 int mbk_inv_diag(const mb_stencil_dev *st, double *d64, float *d32, cudaStream_t s);
+int mbk_stencil_codes(const mb_stencil_dev *st, uint8_t *code, uint16_t *rowid, cudaStream_t s);
 
 #ifdef __cplusplus
 }

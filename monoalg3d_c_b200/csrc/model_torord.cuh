@@ -66,6 +66,18 @@ struct TorRhs {
 template <typename T>
 __device__ __forceinline__ T sq(T x) { return x * x; }
 
+// x / (exp(x) - 1), with its limit 1 - x/2 near x = 0.  The GHK fluxes
+// divide by exp(z V F/RT) - 1, which vanishes at V = 0; in single precision
+// exp(x) rounds to 1 once |V| is below a few microvolts and the quotient
+// becomes 0/0, which a travelling wave crossing 0 mV in a million cells meets
+// about once per beat.  The single-precision form therefore evaluates the
+// flux through this function (the plain FP64 form keeps the reference's
+// expression, whose singularity double precision does not reach).
+__device__ __forceinline__ float ghk_b(float x) {
+    if (fabsf(x) < 1e-4f) return 1.0f - 0.5f * x;
+    return x / mexpm1(x);
+}
+
 // Activity-coefficient factor exp(-A z^2 (sqrt(I)/(1+sqrt(I)) - 0.3 I)).
 template <typename T>
 __device__ __forceinline__ T davies(T z2, T I) {
@@ -262,16 +274,24 @@ __device__ __forceinline__ void torord_rhs(const T *y, T stim, T celltype, const
     const T gamma_kao = gamma_nao;
     const T e2 = mexp(T(2.0) * vfrt);
     const T e1 = mexp(T(1.0) * vfrt);
-    const T PhiCaL_ss = T(4.0) * vffrt * (gamma_cai * cass * e2 - gamma_cao * cao) / (e2 - T(1.0));
-    const T PhiCaNa_ss = T(1.0) * vffrt * (gamma_nai * nass * e1 - gamma_nao * nao) / (e1 - T(1.0));
-    const T PhiCaK_ss = T(1.0) * vffrt * (gamma_ki * kss * e1 - gamma_kao * ko) / (e1 - T(1.0));
+    // q1 = vffrt / (e1 - 1), q2 = vffrt / (e2 - 1); used by the FP32 form only
+    T q1 = T(0), q2 = T(0);
+    if constexpr (sizeof(T) == 4) {
+        q1 = F * ghk_b(vfrt);
+        q2 = T(0.5) * F * ghk_b(T(2.0) * vfrt);
+    }
+    // z2x * vffrt * num / (e - 1), the reference's form in FP64
+#define MB_GHK(z2x, num, e, q) (sizeof(T) == 8 ? (z2x) * vffrt * (num) / ((e) - T(1.0)) : (z2x) * (q) * (num))
+    const T PhiCaL_ss = MB_GHK(T(4.0), gamma_cai * cass * e2 - gamma_cao * cao, e2, q2);
+    const T PhiCaNa_ss = MB_GHK(T(1.0), gamma_nai * nass * e1 - gamma_nao * nao, e1, q1);
+    const T PhiCaK_ss = MB_GHK(T(1.0), gamma_ki * kss * e1 - gamma_kao * ko, e1, q1);
     Ii = T(0.5) * (nai + ki + cli + T(4) * cai) / T(1000);
     gamma_cai = davies(T(4), Ii);
     gamma_nai = davies(T(1), Ii);
     gamma_ki = davies(T(1), Ii);
-    const T PhiCaL_i = T(4.0) * vffrt * (gamma_cai * cai * e2 - gamma_cao * cao) / (e2 - T(1.0));
-    const T PhiCaNa_i = T(1.0) * vffrt * (gamma_nai * nai * e1 - gamma_nao * nao) / (e1 - T(1.0));
-    const T PhiCaK_i = T(1.0) * vffrt * (gamma_ki * ki * e1 - gamma_kao * ko) / (e1 - T(1.0));
+    const T PhiCaL_i = MB_GHK(T(4.0), gamma_cai * cai * e2 - gamma_cao * cao, e2, q2);
+    const T PhiCaNa_i = MB_GHK(T(1.0), gamma_nai * nai * e1 - gamma_nao * nao, e1, q1);
+    const T PhiCaK_i = MB_GHK(T(1.0), gamma_ki * ki * e1 - gamma_kao * ko, e1, q1);
 
     T PCa = T(8.3757e-05) * sc.ICaL;
     if (EPI) PCa = PCa * T(1.2);
@@ -397,9 +417,11 @@ __device__ __forceinline__ void torord_rhs(const T *y, T stim, T celltype, const
     if (EPI) GKb = GKb * T(0.6);
     const T IKb = GKb * xkb * (v - EK);
     const T PNab = T(1.9239e-09);
-    const T INab = PNab * vffrt * (nai * e1 - nao) / (e1 - T(1.0));
+    const T INab = sizeof(T) == 8 ? PNab * vffrt * (nai * e1 - nao) / (e1 - T(1.0)) : PNab * q1 * (nai * e1 - nao);
     const T PCab = T(5.9194e-08);
-    const T ICab = PCab * T(4.0) * vffrt * (gamma_cai * cai * e2 - gamma_cao * cao) / (e2 - T(1.0));
+    const T ICab = sizeof(T) == 8 ? PCab * T(4.0) * vffrt * (gamma_cai * cai * e2 - gamma_cao * cao) / (e2 - T(1.0))
+                                  : PCab * T(4.0) * q2 * (gamma_cai * cai * e2 - gamma_cao * cao);
+#undef MB_GHK
     const T GpCa = T(5e-04);
     const T IpCa = GpCa * cai / (T(0.0005) + cai);
 

@@ -251,6 +251,9 @@ struct mb_monodomain {
     double *d_fx, *d_fy, *d_fz;
     double *d_table;
     float *d_table32;
+    uint8_t *d_code;      /* per-cell coupling codes (kinds 0, 1) */
+    uint16_t *d_rowid;    /* per-cell class-table rows (kind 2)   */
+    float *d_act;         /* activation tracking rows, or NULL    */
     double *d_stim_host;
     mb_ctrl *d_ctrl;
     mb_step_stats *d_log;
@@ -295,6 +298,9 @@ void mb_monodomain_desc_defaults(mb_monodomain_desc *d) {
     d->cg_max_iterations = 200;
     d->use_preconditioner = 1;
     d->initial_v = NAN;
+    d->track_activation = 0;
+    d->activation_threshold = -30.0;
+    d->activation_min_interval = 10.0;
 }
 
 /* alpha = ((beta * cm) / dt) * UM2_TO_CM2 * (dx dy dz), with UM2_TO_CM2 the
@@ -318,7 +324,8 @@ void mb_monodomain_destroy(mb_monodomain *m) {
     void *bufs[] = {m->d_pb, m->d_ppart, m->d_pb32, m->d_bar, m->d_status, m->d_invd, m->d_invd32, m->d_z, m->d_z32,
                     m->d_mask, m->d_cells, m->d_v, m->d_vstar, m->d_r, m->d_p, m->d_r32, m->d_p32,
                     m->d_partials, m->d_sv64, m->d_sv32, m->d_stim_bits, m->d_celltype, m->d_scale,
-                    m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_stim_host, m->d_ctrl, m->d_log};
+                    m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_code, m->d_rowid, m->d_act,
+                    m->d_stim_host, m->d_ctrl, m->d_log};
     for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
     for (int i = 0; i < 4; ++i) if (m->ev[i]) cudaEventDestroy(m->ev[i]);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -615,6 +622,16 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         free(t32);
         m->st.table = m->d_table; m->st.table32 = m->d_table32;
     }
+    /* per-cell row codes read by the persistent CG */
+    if (m->st.kind == 2) {
+        if ((int64_t)d->nz * 9 > 65535) { rc = set_err(MB_ERR_UNSUPPORTED, "nz above 7281 for a per-plane operator"); goto fail; }
+        ALLOC(m->d_rowid, (size_t)n * sizeof(uint16_t));
+    } else {
+        ALLOC(m->d_code, (size_t)n);
+    }
+    m->st.code = m->d_code;
+    m->st.rowid = m->d_rowid;
+    CKK(mbk_stencil_codes(&m->st, m->d_code, m->d_rowid, m->stream));
 
     /* CG work vectors */
     m->cg.precision = d->precision;
@@ -707,6 +724,27 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         }
     }
 
+    /* activation tracking rows (read and written by the ODE kernels) */
+    if (d->track_activation) {
+        const size_t ld = m->ode.ld, bytes = (size_t)MB_ACT_ROWS * ld * sizeof(float);
+        float *h = (float *)malloc(bytes);
+        if (!h) { rc = set_err(MB_ERR_NOMEM, "host memory"); goto fail; }
+        for (size_t q = 0; q < ld; ++q) {
+            h[MB_ACT_VPREV * ld + q] = NAN;
+            h[MB_ACT_FIRST * ld + q] = -1.0f;
+            h[MB_ACT_LAST * ld + q] = -1.0f;
+            h[MB_ACT_APD * ld + q] = -1.0f;
+            h[MB_ACT_VPEAK * ld + q] = 0.0f;
+            h[MB_ACT_VREST * ld + q] = 0.0f;
+            h[MB_ACT_STATE * ld + q] = 0.0f;
+        }
+        cudaError_t e = cudaMalloc((void **)&m->d_act, bytes);
+        if (e == cudaSuccess) e = cudaMemcpy(m->d_act, h, bytes, cudaMemcpyHostToDevice);
+        free(h);
+        if (e != cudaSuccess) { rc = set_err(MB_ERR_NOMEM, "activation rows: %s", cudaGetErrorString(e)); goto fail; }
+        m->ode.act = m->d_act;
+    }
+
     /* control block */
     {
         mb_ctrl c;
@@ -724,6 +762,9 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         c.max_its = d->cg_max_iterations > 0 ? d->cg_max_iterations : 200;
         c.use_precond = d->use_preconditioner ? 1 : 0;
         c.refine_ratio = 1e-8;
+        c.act_dt = d->dt_pde;
+        c.act_threshold = (float)(isnan(d->activation_threshold) ? -30.0 : d->activation_threshold);
+        c.act_min_interval = (float)(isnan(d->activation_min_interval) ? 10.0 : d->activation_min_interval);
         ALLOC(m->d_ctrl, sizeof(mb_ctrl));
         UPLOAD(m->d_ctrl, &c, sizeof c);
         m->pcg.ctrl = m->d_ctrl;
@@ -1080,6 +1121,29 @@ int mb_monodomain_get_state(mb_monodomain *m, double *state_host) {
     CK(cudaMemcpyAsync(state_host, d, bytes, cudaMemcpyDeviceToHost, m->stream));
     CK(cudaStreamSynchronize(m->stream));
     cudaFree(d);
+    return MB_OK;
+}
+
+int mb_monodomain_get_activation(mb_monodomain *m, float *first, float *last, float *apd90, int32_t *count) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    if (!m->d_act) return set_err(MB_ERR_STATE, "activation tracking is off (track_activation = 0)");
+    const size_t ld = m->ode.ld;
+    float *h = (float *)malloc((size_t)MB_ACT_ROWS * ld * sizeof(float));
+    if (!h) return set_err(MB_ERR_NOMEM, "host memory");
+    cudaError_t e = cudaStreamSynchronize(m->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(h, m->d_act, (size_t)MB_ACT_ROWS * ld * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { free(h); return set_err(MB_ERR_CUDA, "%s", cudaGetErrorString(e)); }
+    uint32_t t = 0;
+    for (int64_t g = 0; g < m->n; ++g) {
+        const int on = !m->h_mask || m->h_mask[g];
+        const int st = on ? (int)h[MB_ACT_STATE * ld + t] : 0;
+        if (first) first[g] = on ? h[MB_ACT_FIRST * ld + t] : -1.0f;
+        if (last) last[g] = on ? h[MB_ACT_LAST * ld + t] : -1.0f;
+        if (apd90) apd90[g] = on ? h[MB_ACT_APD * ld + t] : -1.0f;
+        if (count) count[g] = st >> 1;
+        if (on) ++t;
+    }
+    free(h);
     return MB_OK;
 }
 

@@ -44,6 +44,60 @@ __device__ __forceinline__ double cell_stim(const mb_ode_dev &o, const mb_ctrl *
     return s;
 }
 
+// Activation time and APD90 of compact cell t from V at the start of the loop
+// step (time cur_time).  An activation is an upward crossing of
+// act_threshold (the reference's activation_threshold, save_mesh.c:787-848)
+// at least act_min_interval after the previous one (its time_threshold), its
+// time linearly interpolated between the two loop steps.  APD90 ends at the
+// downward crossing, after the peak, of V_peak - 0.9 (V_peak - V_rest) with
+// V_rest the lowest V since the previous repolarisation, also interpolated.
+__device__ __forceinline__ void act_track(const mb_ode_dev &o, const mb_ctrl *__restrict__ c, uint32_t t,
+                                          double Vd) {
+    if (o.act == nullptr || c == nullptr) return;
+    float *a = o.act;
+    const size_t ld = o.ld;
+    const float V = (float)Vd;
+    const float vp = a[MB_ACT_VPREV * ld + t];
+    if (isnan(vp)) {
+        a[MB_ACT_VPREV * ld + t] = V;
+        a[MB_ACT_VREST * ld + t] = V;
+        return;
+    }
+    const double tc = c->cur_time, dt = c->act_dt;
+    int state = (int)a[MB_ACT_STATE * ld + t];
+    int n = state >> 1, phase = state & 1;
+    const float thr = c->act_threshold;
+    if (vp < thr && V >= thr) {
+        const float tl = a[MB_ACT_LAST * ld + t];
+        if (tl < 0.0f || tc - (double)tl > (double)c->act_min_interval) {
+            const float ta = (float)((tc - dt) + dt * (double)(thr - vp) / (double)(V - vp));
+            if (n == 0) a[MB_ACT_FIRST * ld + t] = ta;
+            a[MB_ACT_LAST * ld + t] = ta;
+            a[MB_ACT_APD * ld + t] = -1.0f;
+            a[MB_ACT_VPEAK * ld + t] = V;
+            n += 1;
+            phase = 1;
+        }
+    }
+    if (phase) {
+        const float pk = fmaxf(a[MB_ACT_VPEAK * ld + t], V);
+        a[MB_ACT_VPEAK * ld + t] = pk;
+        const float rest = a[MB_ACT_VREST * ld + t];
+        const float v90 = pk - 0.9f * (pk - rest);
+        if (vp > v90 && V <= v90 && V < pk) {
+            const double tr = (tc - dt) + dt * (double)(vp - v90) / (double)(vp - V);
+            a[MB_ACT_APD * ld + t] = (float)(tr - (double)a[MB_ACT_LAST * ld + t]);
+            a[MB_ACT_VREST * ld + t] = V;
+            phase = 0;
+        }
+    } else {
+        const float rest = a[MB_ACT_VREST * ld + t];
+        if (V < rest) a[MB_ACT_VREST * ld + t] = V;
+    }
+    a[MB_ACT_VPREV * ld + t] = V;
+    a[MB_ACT_STATE * ld + t] = (float)(2 * n + phase);
+}
+
 template <typename T>
 __device__ __forceinline__ TTScale<T> load_tt_scale(const mb_ode_dev &o, uint32_t t) {
     TTScale<T> sc;
@@ -80,6 +134,7 @@ k_tt2006_fp64(mb_ode_dev o, const mb_ctrl *__restrict__ ctrl, const double *__re
     const double *src = (ctrl == nullptr || ctrl->cur_time > 0.0) ? vin : vout;
     double y[TT_NEQ];
     y[0] = src[g];
+    act_track(o, ctrl, t, y[0]);
 #pragma unroll
     for (int s = 1; s < TT_NEQ; ++s) y[s] = o.sv64[s * ld + t];
     const TTScale<double> sc = load_tt_scale<double>(o, t);
@@ -115,6 +170,7 @@ k_tt2006_mixed(mb_ode_dev o, const mb_ctrl *__restrict__ ctrl, const double *__r
     const size_t ld = o.ld;
     const double *src = (ctrl == nullptr || ctrl->cur_time > 0.0) ? vin : vout;
     double V = src[g];
+    act_track(o, ctrl, t, V);
     double cai = o.sv64[1 * ld + t], casr = o.sv64[2 * ld + t], cass = o.sv64[3 * ld + t];
     double nai = o.sv64[4 * ld + t], ki = o.sv64[5 * ld + t];
     float gates[12];
@@ -170,6 +226,7 @@ k_torord_fp64(mb_ode_dev o, const mb_ctrl *__restrict__ ctrl, const double *__re
     const double *src = (ctrl == nullptr || ctrl->cur_time > 0.0) ? vin : vout;
     double y[TOR_NEQ];
     y[0] = src[g];
+    act_track(o, ctrl, t, y[0]);
 #pragma unroll
     for (int s = 1; s < TOR_NEQ; ++s) y[s] = o.sv64[s * ld + t];
     const double celltype = o.celltype ? (double)o.celltype[t] : 0.0;
@@ -196,6 +253,7 @@ k_torord_mixed(mb_ode_dev o, const mb_ctrl *__restrict__ ctrl, const double *__r
     const double *src = (ctrl == nullptr || ctrl->cur_time > 0.0) ? vin : vout;
     TorMixedState st;
     st.d[0] = src[g];
+    act_track(o, ctrl, t, st.d[0]);
 #pragma unroll
     for (int r = 1; r < TOR_N64; ++r) st.d[r] = o.sv64[r * ld + t];
 #pragma unroll

@@ -79,7 +79,8 @@ def build_desc(nx: int, ny: int, nz: int, dx: float = 100.0, dy: float = 100.0, 
                celltype: Optional[np.ndarray] = None, current_scale: Optional[np.ndarray] = None,
                initial_state: Optional[np.ndarray] = None, cg_tolerance: float = 1e-16,
                cg_max_iterations: int = 200, use_preconditioner: bool = True,
-               stims: Sequence[Stim] = (), initial_v: float = float("nan")) -> Tuple[MbDesc, list]:
+               stims: Sequence[Stim] = (), initial_v: float = float("nan"), track_activation: bool = False,
+               activation_threshold: float = -30.0, activation_min_interval: float = 10.0) -> Tuple[MbDesc, list]:
     """The C-ABI tissue description (mb_monodomain_desc) for these arguments,
     with the arrays it points to (keep them alive while the description is
     in use).  Arrays given per cell are in grid order."""
@@ -131,6 +132,9 @@ def build_desc(nx: int, ny: int, nz: int, dx: float = 100.0, dy: float = 100.0, 
             t.max[a] = s.max[a]
         t.cell_mask = arr(s.cell_mask, np.uint8, n)
     d.initial_v = initial_v
+    d.track_activation = 1 if track_activation else 0
+    d.activation_threshold = activation_threshold
+    d.activation_min_interval = activation_min_interval
     return d, keep
 
 
@@ -150,7 +154,8 @@ class Tissue:
                  celltype: Optional[np.ndarray] = None, current_scale: Optional[np.ndarray] = None,
                  initial_state: Optional[np.ndarray] = None, cg_tolerance: float = 1e-16,
                  cg_max_iterations: int = 200, use_preconditioner: bool = True,
-                 stims: Sequence[Stim] = (), initial_v: float = float("nan")):
+                 stims: Sequence[Stim] = (), initial_v: float = float("nan"), track_activation: bool = False,
+                 activation_threshold: float = -30.0, activation_min_interval: float = 10.0):
         self.shape = (nz, ny, nx)
         self.n = nx * ny * nz
         d, keep = build_desc(nx, ny, nz, dx, dy, dz, active=active, dt_pde=dt_pde, dt_ode=dt_ode, beta=beta,
@@ -159,7 +164,9 @@ class Tissue:
                              fibre_angle_z=fibre_angle_z, sigma_cell=sigma_cell, celltype=celltype,
                              current_scale=current_scale, initial_state=initial_state,
                              cg_tolerance=cg_tolerance, cg_max_iterations=cg_max_iterations,
-                             use_preconditioner=use_preconditioner, stims=stims, initial_v=initial_v)
+                             use_preconditioner=use_preconditioner, stims=stims, initial_v=initial_v,
+                             track_activation=track_activation, activation_threshold=activation_threshold,
+                             activation_min_interval=activation_min_interval)
         self.model = model
         self.precision = precision
         self.active = None if active is None else np.asarray(active, dtype=bool).reshape(-1).copy()
@@ -218,6 +225,16 @@ class Tissue:
     def set_v(self, v: np.ndarray):
         v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
         check(lib.mb_monodomain_set_v(self._h, _ptr(v)))
+
+    def activation(self) -> dict:
+        """Activation times tracked on the device (needs track_activation):
+        first / last activation time and APD90 of the latest beat in ms (-1
+        where there is none), and the number of activations, per grid cell."""
+        out = {k: np.empty(self.n, dtype=np.float32) for k in ("first", "last", "apd90")}
+        out["count"] = np.empty(self.n, dtype=np.int32)
+        check(lib.mb_monodomain_get_activation(self._h, _ptr(out["first"]), _ptr(out["last"]), _ptr(out["apd90"]),
+                                               _ptr(out["count"])))
+        return out
 
     def info(self):
         count, t, na, neq = C.c_int64(), C.c_double(), C.c_uint32(), C.c_int()

@@ -112,4 +112,27 @@ def config4(scale: float = 1.0) -> Workload:
     return Workload("slab_500x500x100_torord_rotating_fibres", nx, ny, nz, kw, sim_ms=1000.0)
 
 
+def config2_instances(scale: float = 1.0, n_cables: int = 128, n_sheets: int = 128):
+    """The batching configuration's tissues: cables of length uniform 1-4 cm
+    at 100 um (100-400 cells) and square sheets with side uniform 64-256
+    cells, each with log-normal (sigma 0.2, median 1) scalings of gNa, gKr,
+    gKs, gCaL and gK1.  Returns (sizes, scales)."""
+    r = rng(SEED_SCALES)
+    cable_len = np.rint(r.uniform(1.0, 4.0, n_cables) * 100.0 * scale).astype(int)
+    sheet_side = np.rint(r.integers(64, 257, n_sheets) * scale).astype(int)
+    sizes = [(max(2, int(c)), 1) for c in cable_len] + [(max(2, int(s)), max(2, int(s))) for s in sheet_side]
+    scales = np.exp(0.2 * r.standard_normal((len(sizes), 5)))
+    return sizes, scales
+
+
+def config2(scale: float = 1.0):
+    """Batching: 256 independent tissues (128 cables, 128 sheets), TT2006 with
+    per-tissue scalings, isotropic 0.13 S/m, stimulus on the x = 0 edge,
+    400 ms; outputs activation time and APD90 per cell.  Returns the batch's
+    sizes, scales and Tissue keywords."""
+    sizes, scales = config2_instances(scale)
+    kw = dict(model="tt2006", assembly="homogeneous", sigma=(0.13 * S_PER_M,) * 3, track_activation=True)
+    return sizes, scales, kw
+
+
 CONFIGS = {0: config0, 1: config1, 4: config4}

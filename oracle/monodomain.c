@@ -97,7 +97,8 @@ int orc_create(orc_sim **out, const mb_monodomain_desc *d) {
         s->scale = malloc(sizeof(double) * (size_t)n * MB_NUM_SCALES);
         if (!s->scale) { orc_destroy(s); return MB_ERR_NOMEM; }
         for (int32_t c = 0; c < n; ++c)
-            for (int q = 0; q < MB_NUM_SCALES; ++q) s->scale[(size_t)c * MB_NUM_SCALES + q] = d->current_scale[q * ng + s->cells[c]];
+            for (int q = 0; q < MB_NUM_SCALES; ++q)  /* the device keeps the scalings as float */
+                s->scale[(size_t)c * MB_NUM_SCALES + q] = (double)(float)d->current_scale[q * ng + s->cells[c]];
     }
     s->alpha = (((d->beta * d->cm) / d->dt_pde) * (double)1.0e-8f) * (d->dx * d->dy * d->dz);
     s->num_steps = (int)(d->dt_pde / d->dt_ode);

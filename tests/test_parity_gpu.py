@@ -67,7 +67,9 @@ def test_split_api_matches_whole_step():
         its, err = b.conjugate_gradient()
         assert its >= 1 and err <= 1e-16
         b.advance_time()
-    np.testing.assert_array_equal(a.v(), b.v())
+    # the two tissues may have tuned different CG launch shapes (another
+    # summation order), so equal to rounding rather than bit for bit
+    np.testing.assert_allclose(a.v(), b.v(), rtol=1e-12, atol=1e-12)
     assert b.info()["count"] == 60
 
 
