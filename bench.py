@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 4])
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 4])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

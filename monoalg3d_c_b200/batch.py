@@ -30,6 +30,29 @@ def pack(sizes: Sequence[Tuple[int, int]]):
     return W.value, H.value, x0, y0
 
 
+def atlas(sizes: Sequence[Tuple[int, int]], scales: Optional[np.ndarray], stim: Stim, dx: float = 100.0):
+    """(atlas_nx, atlas_ny, x0, y0, Tissue keywords) of the atlas holding the
+    tissues: the active mask, per-cell scalings and the stimulus mask."""
+    sizes = [(int(a), int(b)) for a, b in sizes]
+    W, H, x0, y0 = pack(sizes)
+    n = W * H
+    active = np.zeros((H, W), dtype=np.uint8)
+    stim_mask = np.zeros((H, W), dtype=np.uint8)
+    scale = np.ones((MB_NUM_SCALES, H, W), dtype=np.float64)
+    for q, (nx, ny) in enumerate(sizes):
+        sl = (slice(y0[q], y0[q] + ny), slice(x0[q], x0[q] + nx))
+        active[sl] = 1
+        cx = (np.arange(nx) + 0.5) * dx
+        stim_mask[sl] = (cx < stim.x_limit)[None, :]
+        if scales is not None:
+            scale[(slice(None),) + sl] = np.asarray(scales[q], dtype=np.float64)[:, None, None]
+    stims = [Stim(kind="cell_mask", start=stim.start, duration=stim.duration, current=stim.current,
+                  period=stim.period, cell_mask=stim_mask.reshape(-1))]
+    kw = dict(active=active.reshape(-1), stims=stims,
+              current_scale=None if scales is None else scale.reshape(MB_NUM_SCALES, n))
+    return W, H, x0, y0, kw
+
+
 class Batch:
     """Independent 2-D tissues (sheets, cables) solved in one atlas tissue.
 
@@ -44,26 +67,12 @@ class Batch:
                  stim: Stim = Stim(kind="x_less_than", start=0.0, duration=2.0, current=-53.0, x_limit=100.0),
                  dx: float = 100.0, **kw):
         self.sizes = [(int(a), int(b)) for a, b in sizes]
-        W, H, x0, y0 = pack(self.sizes)
+        W, H, x0, y0, akw = atlas(self.sizes, scales, stim, dx)
         self.atlas = (W, H)
         self.x0, self.y0 = x0, y0
-        n = W * H
-        active = np.zeros((H, W), dtype=np.uint8)
-        stim_mask = np.zeros((H, W), dtype=np.uint8)
-        scale = np.ones((MB_NUM_SCALES, H, W), dtype=np.float64)
-        for q, (nx, ny) in enumerate(self.sizes):
-            sl = (slice(y0[q], y0[q] + ny), slice(x0[q], x0[q] + nx))
-            active[sl] = 1
-            cx = (np.arange(nx) + 0.5) * dx
-            stim_mask[sl] = (cx < stim.x_limit)[None, :]
-            if scales is not None:
-                scale[(slice(None),) + sl] = np.asarray(scales[q], dtype=np.float64)[:, None, None]
-        self.active_cells = int(active.sum())
-        stims = [Stim(kind="cell_mask", start=stim.start, duration=stim.duration, current=stim.current,
-                      period=stim.period, cell_mask=stim_mask.reshape(-1))]
-        self.tissue = Tissue(W, H, 1, dx, dx, dx, active=active.reshape(-1),
-                             current_scale=None if scales is None else scale.reshape(MB_NUM_SCALES, n),
-                             stims=stims, **kw)
+        self.active_cells = int(akw["active"].sum())
+        akw.update(kw)
+        self.tissue = Tissue(W, H, 1, dx, dx, dx, **akw)
 
     def split(self, grid: np.ndarray) -> List[np.ndarray]:
         """Per-tissue (ny, nx) views of an atlas array in grid order."""

@@ -135,4 +135,17 @@ def config2(scale: float = 1.0):
     return sizes, scales, kw
 
 
-CONFIGS = {0: config0, 1: config1, 4: config4}
+def config2_workload(scale: float = 1.0) -> Workload:
+    """The batching configuration as one atlas tissue (mb_batch_pack): the
+    256 tissues side by side with removed cells between them."""
+    from .batch import atlas
+    sizes, scales, kw = config2(scale)
+    W, H, x0, y0, akw = atlas(sizes, scales, Stim(kind="x_less_than", start=0.0, duration=2.0, current=-53.0,
+                                                  x_limit=100.0))
+    kw = dict(kw)
+    kw.update(akw)
+    return Workload("batch_256_cables_and_sheets_tt2006", W, H, 1, kw, sim_ms=400.0,
+                    note=f"{len(sizes)} tissues in a {W}x{H} atlas")
+
+
+CONFIGS = {0: config0, 1: config1, 2: config2_workload, 4: config4}
