@@ -274,33 +274,298 @@ __device__ __forceinline__ typename Prec<MIXED>::T inv_d(const Args &a, uint32_t
     else return a.inv_diag64[g];
 }
 
+// ---- four cells per thread ----------------------------------------------------
+//
+// With nx a multiple of 4, a thread takes 4 consecutive cells of an x-row
+// (a group, first index g0 a multiple of 4) and reads every row of the
+// stencil as one 16-byte load (two for doubles): the group itself, the rows
+// at -y, +y, -z, +z (kind 2: the nine rows dy, dz in -1..1), plus one scalar
+// on each side for the x neighbours of the group's end cells.  Row indices
+// are clamped into the grid; values of neighbours that do not couple are
+// discarded (kinds 0, 1) or multiplied by the zero coefficients the class
+// table holds for them (kind 2).  Sums run in the same order as the
+// one-cell-per-thread rows above, so both forms give the same values.
+
+template <typename T>
+struct Vec4 { T v[4]; };
+
+__device__ __forceinline__ Vec4<float> ld4(const float *p, uint32_t i) {
+    const float4 f = *reinterpret_cast<const float4 *>(p + i);
+    return {{f.x, f.y, f.z, f.w}};
+}
+__device__ __forceinline__ Vec4<double> ld4(const double *p, uint32_t i) {
+    const double2 a = *reinterpret_cast<const double2 *>(p + i);
+    const double2 b = *reinterpret_cast<const double2 *>(p + i + 2);
+    return {{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ void st4(float *p, uint32_t i, const Vec4<float> &v) {
+    *reinterpret_cast<float4 *>(p + i) = make_float4(v.v[0], v.v[1], v.v[2], v.v[3]);
+}
+__device__ __forceinline__ void st4(double *p, uint32_t i, const Vec4<double> &v) {
+    *reinterpret_cast<double2 *>(p + i) = make_double2(v.v[0], v.v[1]);
+    *reinterpret_cast<double2 *>(p + i + 2) = make_double2(v.v[2], v.v[3]);
+}
+
+// Field readers: row(i) = the 4 values at i..i+3 (i a multiple of 4), at(i) =
+// one value.
+template <typename T>
+struct Plain {
+    const T *f;
+    __device__ __forceinline__ Vec4<T> row(uint32_t i) const { return ld4(f, i); }
+    __device__ __forceinline__ T at(uint32_t i) const { return f[i]; }
+};
+// p_new = z + beta p_old, formed where it is read.
+template <typename T>
+struct Direction {
+    const T *z, *p;
+    T beta;
+    __device__ __forceinline__ Vec4<T> row(uint32_t i) const {
+        const Vec4<T> a = ld4(z, i), b = ld4(p, i);
+        Vec4<T> o;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) o.v[k] = a.v[k] + beta * b.v[k];
+        return o;
+    }
+    __device__ __forceinline__ T at(uint32_t i) const { return z[i] + beta * p[i]; }
+};
+
+// (A f) for the group at g0: pc = f at the 4 cells, ap = the products, m =
+// the cells' code bytes (kind 2: all active).
+template <typename T, int KIND, typename F>
+__device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, const F &f, Vec4<T> &pc, Vec4<T> &ap,
+                                       unsigned (&m)[4]) {
+    const uint32_t sy = (uint32_t)st.nx, sz = (uint32_t)st.nx * (uint32_t)st.ny, n = sz * (uint32_t)st.nz;
+    pc = f.row(g0);
+    if constexpr (KIND == 2) {
+        const ushort4 rid = *reinterpret_cast<const ushort4 *>(st.rowid + g0);
+        const size_t rw[4] = {(size_t)rid.x * 27, (size_t)rid.y * 27, (size_t)rid.z * 27, (size_t)rid.w * 27};
+        T acc[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy) {
+                uint32_t b = g0;
+                if (dz < 0) b = b >= sz ? b - sz : g0;
+                if (dz > 0) b = b + sz < n ? b + sz : g0;
+                if (dy < 0) b = b >= sy ? b - sy : g0;
+                if (dy > 0) b = b + sy < n ? b + sy : g0;
+                const Vec4<T> mid = (dz == 0 && dy == 0) ? pc : f.row(b);
+                T w[6];
+                w[0] = f.at(b > 0 ? b - 1 : b);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) w[k + 1] = mid.v[k];
+                w[5] = f.at(b + 4 < n ? b + 4 : b);
+#pragma unroll
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int q = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const T c = sizeof(T) == 8 ? T(__ldg(st.table + rw[k] + q)) : T(__ldg(st.table32 + rw[k] + q));
+                        acc[k] += c * w[k + 1 + dx];
+                    }
+                }
+            }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            ap.v[k] = acc[k];
+            m[k] = ACTIVE;
+        }
+    } else {
+        const uchar4 cd = *reinterpret_cast<const uchar4 *>(st.code + g0);
+        m[0] = cd.x; m[1] = cd.y; m[2] = cd.z; m[3] = cd.w;
+        const T xl = f.at(g0 > 0 ? g0 - 1 : g0), xr = f.at(g0 + 4 < n ? g0 + 4 : g0);
+        const Vec4<T> ym = f.row(g0 >= sy ? g0 - sy : g0), yp = f.row(g0 + sy < n ? g0 + sy : g0);
+        const Vec4<T> zm = f.row(g0 >= sz ? g0 - sz : g0), zp = f.row(g0 + sz < n ? g0 + sz : g0);
+        T c[6][4];
+        if constexpr (KIND == 0) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                c[0][k] = c[1][k] = T(st.cx);
+                c[2][k] = c[3][k] = T(st.cy);
+                c[4][k] = c[5][k] = T(st.cz);
+            }
+        } else {
+            const Vec4<double> fx = ld4(st.fx, g0), fy = ld4(st.fy, g0), fz = ld4(st.fz, g0);
+            const Vec4<double> fym = ld4(st.fy, g0 >= sy ? g0 - sy : g0), fzm = ld4(st.fz, g0 >= sz ? g0 - sz : g0);
+            const double fxl = __ldg(st.fx + (g0 > 0 ? g0 - 1 : g0));
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                c[0][k] = T(k ? fx.v[k - 1] : fxl);
+                c[1][k] = T(fx.v[k]);
+                c[2][k] = T(fym.v[k]);
+                c[3][k] = T(fy.v[k]);
+                c[4][k] = T(fzm.v[k]);
+                c[5][k] = T(fz.v[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const T p = pc.v[k];
+            const T nb[6] = {k ? pc.v[k - 1] : xl, k < 3 ? pc.v[k + 1] : xr, ym.v[k], yp.v[k], zm.v[k], zp.v[k]};
+            T acc = T(st.alpha) * p;
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                if ((m[k] >> q) & 1u) acc += c[q][k] * (p - nb[q]);
+            ap.v[k] = acc;
+        }
+    }
+}
+
+// A pass over the groups of the block's range: act(g0, pc, ap, m) per group.
+template <typename T, int KIND, int NT, typename F, typename ACT>
+__device__ __forceinline__ void pass4(const mb_stencil_dev &st, const F &f, ACT act) {
+    const uint32_t groups = ((uint32_t)st.nx * st.ny * st.nz) >> 2;
+    uint32_t c0, c1;
+    block_chunk(groups, c0, c1);
+    for (uint32_t q = c0 + threadIdx.x; q < c1; q += NT) {
+        const uint32_t g0 = q << 2;
+        Vec4<T> pc, ap;
+        unsigned m[4];
+        apply4<T, KIND>(st, g0, f, pc, ap, m);
+        act(g0, pc, ap, m);
+    }
+}
+
+// ---- the three passes, for either layout ---------------------------------------
+
 // FP64 true residual r = b - A x; stores r (in T), z and p = z; accumulates
 // r.z (T products, FP64 sums), r.r of the stored r, and the FP64 r.r.
-template <bool MIXED, int KIND, int NT, int U>
+template <bool MIXED, int KIND, int NT, int U, bool VEC>
 __device__ __forceinline__ void residual_pass(const Args &a, typename Prec<MIXED>::T *r,
                                               typename Prec<MIXED>::T *p, bool pre, double (&acc)[3]) {
     using T = typename Prec<MIXED>::T;
     const mb_stencil_dev &st = a.st;
     const double *__restrict__ x = a.x;
-    pass<double, KIND, NT, U>(st, [&](uint32_t q) { return x[q]; },
-                              [&](uint32_t g, const auto &row) {
-                                  const double ax = product<double, KIND>(st, row);
-                                  const double bb = a.b ? a.b[g] : st.alpha * a.vstar[g];
-                                  const double r64 = bb - ax;
-                                  const T rt = (T)r64;
-                                  const T z = pre ? inv_d<MIXED>(a, g) * rt : rt;
-                                  r[g] = rt;
-                                  p[g] = z;
-                                  acc[0] += (double)rt * (double)z;
-                                  acc[1] += (double)rt * (double)rt;
-                                  acc[2] += r64 * r64;
-                              });
+    if constexpr (VEC) {
+        pass4<double, KIND, NT>(st, Plain<double>{x}, [&](uint32_t g0, const Vec4<double> &xc, const Vec4<double> &ax,
+                                                        const unsigned (&m)[4]) {
+            Vec4<T> rv = ld4(r, g0), pv = ld4(p, g0);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (!(m[k] & ACTIVE)) continue;
+                const uint32_t g = g0 + k;
+                const double bb = a.b ? a.b[g] : st.alpha * a.vstar[g];
+                const double r64 = bb - ax.v[k];
+                const T rt = (T)r64;
+                const T z = pre ? inv_d<MIXED>(a, g) * rt : rt;
+                rv.v[k] = rt;
+                pv.v[k] = z;
+                acc[0] += (double)rt * (double)z;
+                acc[1] += (double)rt * (double)rt;
+                acc[2] += r64 * r64;
+            }
+            st4(r, g0, rv);
+            st4(p, g0, pv);
+        });
+    } else {
+        pass<double, KIND, NT, U>(st, [&](uint32_t q) { return x[q]; },
+                                  [&](uint32_t g, const auto &row) {
+                                      const double ax = product<double, KIND>(st, row);
+                                      const double bb = a.b ? a.b[g] : st.alpha * a.vstar[g];
+                                      const double r64 = bb - ax;
+                                      const T rt = (T)r64;
+                                      const T z = pre ? inv_d<MIXED>(a, g) * rt : rt;
+                                      r[g] = rt;
+                                      p[g] = z;
+                                      acc[0] += (double)rt * (double)z;
+                                      acc[1] += (double)rt * (double)rt;
+                                      acc[2] += r64 * r64;
+                                  });
+    }
 }
 
-template <bool MIXED, int KIND, int NT, int U, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
+// Q: the direction (p_new = z + beta p_old, or p itself on a restart), stored
+// when new, and the partial sum of p.Ap.
+template <bool MIXED, int KIND, int NT, int U, bool VEC>
+__device__ __forceinline__ void q_pass(const Args &a, bool first, const typename Prec<MIXED>::T *po,
+                                       typename Prec<MIXED>::T *pw, const typename Prec<MIXED>::T *zb, double beta,
+                                       double &q1) {
     using T = typename Prec<MIXED>::T;
     const mb_stencil_dev &st = a.st;
+    const T bt = (T)beta;
+    if constexpr (VEC) {
+        auto dot = [&](const Vec4<T> &pc, const Vec4<T> &ap, const unsigned (&m)[4]) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (m[k] & ACTIVE) q1 += (double)pc.v[k] * (double)ap.v[k];
+        };
+        if (first) {
+            pass4<T, KIND, NT>(st, Plain<T>{po}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
+                                                     const unsigned (&m)[4]) { dot(pc, ap, m); });
+        } else {
+            pass4<T, KIND, NT>(st, Direction<T>{zb, po, bt}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
+                                                                 const unsigned (&m)[4]) {
+                st4(pw, g0, pc);
+                dot(pc, ap, m);
+            });
+        }
+    } else {
+        if (first) {
+            pass<T, KIND, NT, U>(st, [&](uint32_t q) { return po[q]; },
+                                 [&](uint32_t g, const auto &row) {
+                                     q1 += (double)row.pc * (double)product<T, KIND>(st, row);
+                                 });
+        } else {
+            pass<T, KIND, NT, U>(st, [&](uint32_t q) { return zb[q] + bt * po[q]; },
+                                 [&](uint32_t g, const auto &row) {
+                                     pw[g] = row.pc;
+                                     q1 += (double)row.pc * (double)product<T, KIND>(st, row);
+                                 });
+        }
+    }
+}
+
+// U: x += alpha p, r -= alpha A p, z = r / diag; partial sums of r.z and r.r.
+template <bool MIXED, int KIND, int NT, int U, bool VEC>
+__device__ __forceinline__ void u_pass(const Args &a, const typename Prec<MIXED>::T *pc_, typename Prec<MIXED>::T *r,
+                                       typename Prec<MIXED>::T *zb, bool pre, double alpha, double (&u2)[2]) {
+    using T = typename Prec<MIXED>::T;
+    const mb_stencil_dev &st = a.st;
+    const T al = (T)alpha;
+    double *__restrict__ x = a.x;
+    if constexpr (VEC) {
+        pass4<T, KIND, NT>(st, Plain<T>{pc_}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
+                                                  const unsigned (&m)[4]) {
+            Vec4<double> xv = ld4(x, g0);
+            Vec4<T> rv = ld4(r, g0), zv = ld4(zb, g0);
+            Vec4<T> id;
+            if (pre) {
+                if constexpr (MIXED) id = ld4(a.inv_diag32, g0);
+                else id = ld4(a.inv_diag64, g0);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (!(m[k] & ACTIVE)) continue;
+                xv.v[k] += alpha * (double)pc.v[k];
+                const T rn = rv.v[k] - al * ap.v[k];
+                rv.v[k] = rn;
+                const T z = pre ? id.v[k] * rn : rn;
+                zv.v[k] = z;
+                u2[0] += (double)z * (double)rn;
+                u2[1] += (double)rn * (double)rn;
+            }
+            st4(x, g0, xv);
+            st4(r, g0, rv);
+            st4(zb, g0, zv);
+        });
+    } else {
+        pass<T, KIND, NT, U>(st, [&](uint32_t q) { return pc_[q]; },
+                             [&](uint32_t g, const auto &row) {
+                                 const T ap = product<T, KIND>(st, row);
+                                 x[g] += alpha * (double)row.pc;
+                                 const T rn = r[g] - al * ap;
+                                 r[g] = rn;
+                                 const T z = pre ? inv_d<MIXED>(a, g) * rn : rn;
+                                 zb[g] = z;
+                                 u2[0] += (double)z * (double)rn;
+                                 u2[1] += (double)rn * (double)rn;
+                             });
+    }
+}
+
+template <bool MIXED, int KIND, int NT, int U, int MINB, bool VEC>
+__global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
+    using T = typename Prec<MIXED>::T;
     mb_ctrl *c = a.ctrl;
     const bool pre = c->use_precond != 0;
     const double tol = c->tol;
@@ -313,7 +578,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
     int red = 0;
 
     double acc[3] = {0.0, 0.0, 0.0}, s3[3];
-    residual_pass<MIXED, KIND, NT, U>(a, r, bufa, pre, acc);
+    residual_pass<MIXED, KIND, NT, U, VEC>(a, r, bufa, pre, acc);
     if (!grid_reduce<3, NT>(a, acc, s3, red)) return;
     double rz = s3[0], rr = s3[1];
     double error = s3[2], rr_ref = s3[2];
@@ -326,41 +591,14 @@ __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
     while (!done) {
         // Q: direction p_new = z + beta p_old fused with A p_new and p.Ap
         T *pcur = first ? pold : pnew;
-        const T *__restrict__ po = pold;
-        T *__restrict__ pw = pnew;
-        const T bt = (T)beta;
         double q1[1] = {0.0}, s1[1];
-        if (first) {
-            pass<T, KIND, NT, U>(st, [&](uint32_t q) { return po[q]; },
-                                 [&](uint32_t g, const auto &row) {
-                                     q1[0] += (double)row.pc * (double)product<T, KIND>(st, row);
-                                 });
-        } else {
-            pass<T, KIND, NT, U>(st, [&](uint32_t q) { return zb[q] + bt * po[q]; },
-                                 [&](uint32_t g, const auto &row) {
-                                     pw[g] = row.pc;
-                                     q1[0] += (double)row.pc * (double)product<T, KIND>(st, row);
-                                 });
-        }
+        q_pass<MIXED, KIND, NT, U, VEC>(a, first, pold, pnew, zb, beta, q1[0]);
         if (!grid_reduce<1, NT>(a, q1, s1, red)) return;
         const double alpha = (pre ? rz : rr) / s1[0];
-        const T al = (T)alpha;
 
         // U: x += alpha p, r -= alpha A p, z = r / diag
         double u2[2] = {0.0, 0.0}, s2[2];
-        const T *__restrict__ pc_ = pcur;
-        double *__restrict__ x = a.x;
-        pass<T, KIND, NT, U>(st, [&](uint32_t q) { return pc_[q]; },
-                             [&](uint32_t g, const auto &row) {
-                                 const T ap = product<T, KIND>(st, row);
-                                 x[g] += alpha * (double)row.pc;
-                                 const T rn = r[g] - al * ap;
-                                 r[g] = rn;
-                                 const T z = pre ? inv_d<MIXED>(a, g) * rn : rn;
-                                 zb[g] = z;
-                                 u2[0] += (double)z * (double)rn;
-                                 u2[1] += (double)rn * (double)rn;
-                             });
+        u_pass<MIXED, KIND, NT, U, VEC>(a, pcur, r, zb, pre, alpha, u2);
         if (!grid_reduce<2, NT>(a, u2, s2, red)) return;
         its += 1;
         pold = pcur;
@@ -380,7 +618,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
             if (s2[1] <= fmax(tol, ratio * rr_ref) || its >= max_its) {
                 // FP64 true residual replaces the FP32 recurrence; restart from it
                 double t3[3] = {0.0, 0.0, 0.0};
-                residual_pass<MIXED, KIND, NT, U>(a, r, pold, pre, t3);
+                residual_pass<MIXED, KIND, NT, U, VEC>(a, r, pold, pre, t3);
                 if (!grid_reduce<3, NT>(a, t3, s3, red)) return;
                 refinements += 1;
                 error = s3[2];
@@ -485,15 +723,22 @@ __global__ void k_inv_diag(mb_stencil_dev st, double *d64, float *d32) {
 struct Variant {
     const void *fn;
     int threads;
+    int groups;    // 1 = four cells per thread
 };
 
-// (threads per block, cells per thread per round, resident blocks per SM)
-#define MB_VARIANTS(K)                                                                                     \
-    {(const void *)k_fcg<MIXED, K, 1024, 1, 1>, 1024}, {(const void *)k_fcg<MIXED, K, 1024, 1, 2>, 1024}, \
-        {(const void *)k_fcg<MIXED, K, 512, 2, 2>, 512}, {(const void *)k_fcg<MIXED, K, 512, 1, 4>, 512},  \
-        {(const void *)k_fcg<MIXED, K, 256, 2, 4>, 256}
+// (threads per block, cells per thread per round, resident blocks per SM,
+// four-cell groups); the group variants need nx to be a multiple of 4
+#define MB_VARIANTS(K)                                                                                          \
+    {(const void *)k_fcg<MIXED, K, 1024, 1, 1, false>, 1024, 0},                                            \
+        {(const void *)k_fcg<MIXED, K, 1024, 1, 2, false>, 1024, 0},                                        \
+        {(const void *)k_fcg<MIXED, K, 512, 2, 2, false>, 512, 0},                                          \
+        {(const void *)k_fcg<MIXED, K, 512, 1, 4, false>, 512, 0},                                          \
+        {(const void *)k_fcg<MIXED, K, 256, 2, 4, false>, 256, 0},                                          \
+        {(const void *)k_fcg<MIXED, K, 1024, 1, 1, true>, 1024, 1},                                         \
+        {(const void *)k_fcg<MIXED, K, 512, 1, 2, true>, 512, 1},                                           \
+        {(const void *)k_fcg<MIXED, K, 256, 1, 4, true>, 256, 1}
 
-constexpr int NUM_VARIANTS = 5;
+constexpr int NUM_VARIANTS = 8;
 
 template <bool MIXED>
 static Variant variant_of(int kind, int v) {
@@ -516,6 +761,11 @@ using namespace mb::fcg;
 extern "C" int mbk_fcg_variants(int kind) {
     (void)kind;
     return NUM_VARIANTS;
+}
+
+// Whether variant v runs four-cell groups (usable only when nx % 4 == 0).
+extern "C" int mbk_fcg_variant_groups(int v) {
+    return v >= 0 && v < NUM_VARIANTS ? variant(0, 0, v).groups : 0;
 }
 
 // Co-resident blocks of a variant (the grid size of its cooperative launch).

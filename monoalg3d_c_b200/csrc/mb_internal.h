@@ -178,6 +178,7 @@ typedef struct mb_pcg_dev {
     int tiles_x, tiles_y, zchunk, nchunks;
 } mb_pcg_dev;
 int mbk_fcg_variants(int kind);
+int mbk_fcg_variant_groups(int variant);
 int mbk_fcg_max_blocks(int mixed, int kind, int variant);
 int mbk_fcg_launch(const mb_pcg_dev *p, cudaStream_t s);
 int mbk_tcg_max_blocks(int mixed);

@@ -388,7 +388,7 @@ static int cg_autotune(mb_monodomain *m) {
         return set_err(MB_ERR_NOMEM, "CG tuning buffer");
     cudaMemcpyAsync(vsave, m->d_v, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
     float best = 1e30f;
-    int bestc = lo, rc = MB_OK;
+    int bestc = 0, rc = MB_OK;      /* variant 0 runs on every grid */
     for (int cand = lo; cand <= hi && !rc; ++cand) {
         mb_pcg_dev q = m->pcg;
         if (cand < nv) {
@@ -402,6 +402,7 @@ static int cg_autotune(mb_monodomain *m) {
             q.blocks = items < mb ? items : mb;
         }
         if (q.blocks <= 0) continue;
+        if (cand < nv && mbk_fcg_variant_groups(cand) && (m->desc.nx % 4) != 0) continue;
         float tsum = 0;
         for (int rep = 0; rep < 3 && !rc; ++rep) {
             cudaMemcpyAsync(m->d_v, vsave, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);

@@ -1,0 +1,62 @@
+"""Every launch shape of the persistent CG (one cell per thread, U cells per
+thread, four-cell groups, 2.5D tiles) against the CPU oracle on each
+operator kind: constant coefficients with removed cells, per-cell
+conductivity, and the 27-point rows of fibres rotating through the wall.
+The shape the autotuner would pick is forced through MB_CG_VARIANT, which
+the tissue reads when it is created.  Bar: V within 1e-8 relative."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import oracle  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 120
+
+
+def _cases():
+    rng = np.random.default_rng(31)
+    nx, ny, nz = 24, 12, 5
+    n = nx * ny * nz
+    return {
+        "masked": (nx, ny, nz, dict(active=(rng.random(n) >= 0.2).astype(np.uint8), model="torord",
+                                    assembly="anisotropic", sigma_l=0.0002, sigma_t=0.00005)),
+        "per_cell": (nx, ny, nz, dict(assembly="per_cell", sigma_cell=0.00013 * np.exp(0.3 * rng.standard_normal(n)),
+                                      active=(rng.random(n) >= 0.1).astype(np.uint8))),
+        "rotating": (nx, ny, nz, dict(assembly="anisotropic", sigma_l=0.0002, sigma_t=0.00004,
+                                      fibre_angle_z=np.deg2rad(np.linspace(60, -60, nz)))),
+    }
+
+
+@pytest.mark.parametrize("case", ["masked", "per_cell", "rotating"])
+def test_every_launch_shape_matches_oracle(case):
+    from monoalg3d_c_b200 import Stim, Tissue
+    nx, ny, nz, kw = _cases()[case]
+    stims = [Stim(kind="x_less_than", start=0.0, duration=2.0, current=-53.0, x_limit=500.0)]
+    o = oracle.Sim(nx, ny, nz, stims=stims, **kw)
+    o.step(STEPS)
+    ref = o.v()
+    o.close()
+    ok = np.isfinite(ref)
+    nv = 9                                       # 8 flat shapes + the tiled kernel
+    old = os.environ.get("MB_CG_VARIANT")
+    try:
+        for v in range(nv):
+            os.environ["MB_CG_VARIANT"] = str(v)
+            t = Tissue(nx, ny, nz, precision="fp64", stims=stims, **kw)
+            kernel = t.tuning()["cg_kernel"]
+            assert kernel == (100 if v == 8 else v), f"variant {v} not used ({kernel})"
+            t.step(STEPS)
+            got = t.v()
+            t.close()
+            err = np.abs(got[ok] - ref[ok])
+            assert np.all(err <= 1e-8 * np.abs(ref[ok]) + 1e-9), f"{case} variant {v}: max |dV| {err.max():.3e}"
+    finally:
+        if old is None:
+            os.environ.pop("MB_CG_VARIANT", None)
+        else:
+            os.environ["MB_CG_VARIANT"] = old
