@@ -339,6 +339,8 @@ __device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, co
     if constexpr (KIND == 2) {
         const ushort4 rid = *reinterpret_cast<const ushort4 *>(st.rowid + g0);
         const size_t rw[4] = {(size_t)rid.x * 27, (size_t)rid.y * 27, (size_t)rid.z * 27, (size_t)rid.w * 27};
+        // away from the x faces the four cells share one table row
+        const bool uni = rid.x == rid.y && rid.x == rid.z && rid.x == rid.w;
         T acc[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
         for (int dz = -1; dz <= 1; ++dz)
@@ -358,9 +360,11 @@ __device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, co
 #pragma unroll
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int q = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+                    const T c0 = sizeof(T) == 8 ? T(__ldg(st.table + rw[0] + q)) : T(__ldg(st.table32 + rw[0] + q));
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        const T c = sizeof(T) == 8 ? T(__ldg(st.table + rw[k] + q)) : T(__ldg(st.table32 + rw[k] + q));
+                        T c = c0;
+                        if (k && !uni) c = sizeof(T) == 8 ? T(__ldg(st.table + rw[k] + q)) : T(__ldg(st.table32 + rw[k] + q));
                         acc[k] += c * w[k + 1 + dx];
                     }
                 }

@@ -762,7 +762,13 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         c.tol = d->cg_tolerance;
         c.max_its = d->cg_max_iterations > 0 ? d->cg_max_iterations : 200;
         c.use_precond = d->use_preconditioner ? 1 : 0;
-        c.refine_ratio = 1e-8;
+        /* the FP32 recurrence is trusted down to refine_ratio x the last
+         * FP64 r.r; MB_REFINE_RATIO overrides it (tuning) */
+        c.refine_ratio = 1e-10;
+        {
+            const char *env = getenv("MB_REFINE_RATIO");
+            if (env && atof(env) > 0.0) c.refine_ratio = atof(env);
+        }
         c.act_dt = d->dt_pde;
         c.act_threshold = (float)(isnan(d->activation_threshold) ? -30.0 : d->activation_threshold);
         c.act_min_interval = (float)(isnan(d->activation_min_interval) ? 10.0 : d->activation_min_interval);
