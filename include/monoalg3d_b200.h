@@ -262,6 +262,28 @@ int mb_monodomain_get_activation(mb_monodomain *m, float *first, float *last, fl
  * 0 <= i' < nx[i], 0 <= j' < ny[i].  Shelf packing, tallest first.          */
 int mb_batch_pack(int n, const int *nx, const int *ny, int *atlas_nx, int *atlas_ny, int *x0, int *y0);
 
+/* ---- discrete adjoint ----------------------------------------------------
+ * No counterpart in the reference.  Gradient of a scalar function of the V
+ * traces at sensor cells with respect to the per-cell conductivity and the
+ * per-cell gKr scaling, by the discrete adjoint of the loop: the transposed
+ * Jacobian of each Rush-Larsen step and a transposed (here: the same,
+ * symmetric) PCG solve per step, run backwards over checkpoints of the loop
+ * state taken every checkpoint_every steps, the states in between recomputed.
+ * The tissue (d) must be ten Tusscher 2006, FP64, per-cell conductivity
+ * (MB_ASSEMBLY_PER_CELL_SIGMA), with conductance scalings and dt_ode = dt_pde.
+ * Samples: V at the sensors after every sample_every steps
+ * (nsteps / sample_every samples).                                          */
+typedef struct mb_adjoint mb_adjoint;
+int mb_adjoint_create(mb_adjoint **out, const mb_monodomain_desc *d, int nsteps, int checkpoint_every,
+                      int n_sensors, const int64_t *sensor_cells, int sample_every);
+/* Runs the loop from the initial state with new conductivities and scalings
+ * (grid order; NULL keeps the current ones); traces: samples x sensors.      */
+int mb_adjoint_forward(mb_adjoint *a, const double *sigma_cell, const double *scale, double *traces);
+/* Given dL/dtraces (samples x sensors), the gradients with respect to
+ * sigma_cell and to the gKr scaling (row 1 of the scalings), grid order.     */
+int mb_adjoint_backward(mb_adjoint *a, const double *dtraces, double *grad_sigma, double *grad_scale_gkr);
+void mb_adjoint_destroy(mb_adjoint *a);
+
 /* Device pointers to V (double, grid order) and to the CUDA stream used. */
 int mb_monodomain_device_v(mb_monodomain *m, double **v_dev, void **stream);
 /* Average duration of the last kernel launches per kind, from CUDA events

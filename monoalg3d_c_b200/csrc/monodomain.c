@@ -19,6 +19,7 @@
 
 #include "mb_internal.h"
 #include "mb_assembly.h"
+#include "mb_tissue.h"
 
 /* ---- error reporting ----------------------------------------------------- */
 
@@ -229,58 +230,7 @@ int mb_ode_set_state(mb_ode *o, const double *host_state) {
 
 /* ---- monodomain tissue --------------------------------------------------- */
 
-struct mb_monodomain {
-    mb_monodomain_desc desc;
-    int neq;
-    int num_steps;
-    int64_t n;            /* grid cells */
-    uint32_t n_active;
-    cudaStream_t stream;
-
-    uint8_t *d_mask;
-    uint32_t *d_cells;
-    double *d_v, *d_vstar;
-    double *d_r, *d_p;
-    float *d_r32, *d_p32;
-    double *d_partials;
-    double *d_sv64;
-    float *d_sv32;
-    uint8_t *d_stim_bits;
-    uint8_t *d_celltype;
-    float *d_scale;
-    double *d_fx, *d_fy, *d_fz;
-    double *d_table;
-    float *d_table32;
-    uint8_t *d_code;      /* per-cell coupling codes (kinds 0, 1) */
-    uint16_t *d_rowid;    /* per-cell class-table rows (kind 2)   */
-    float *d_act;         /* activation tracking rows, or NULL    */
-    double *d_stim_host;
-    mb_ctrl *d_ctrl;
-    mb_step_stats *d_log;
-    int64_t log_len;
-    uint8_t *h_mask;      /* owned copy of desc.active (NULL = all active) */
-    /* persistent CG */
-    int use_pcg;
-    mb_pcg_dev pcg;
-    double *d_pb, *d_ppart, *d_invd, *d_z;
-    float *d_pb32, *d_invd32, *d_z32;
-    unsigned *d_bar;
-    int *d_status;
-    float cg_tune_ms;     /* device time of one CG solve of the chosen kernel at tuning */
-
-    mb_ode_dev ode;
-    mb_stencil_dev st;
-    mb_cg_dev cg;
-
-    cudaGraph_t g_pre, g_body_owner_unused, g_post;
-    cudaGraph_t g_step;
-    cudaGraphExec_t ge_step;
-    cudaGraph_t g_cg;
-    cudaGraphExec_t ge_cg;
-    int use_graphs;
-    int phase;            /* split-API state: 0 idle, 1 ODE done, 2 RHS formed */
-    cudaEvent_t ev[4];
-};
+/* struct mb_monodomain: mb_tissue.h */
 
 void mb_monodomain_desc_defaults(mb_monodomain_desc *d) {
     memset(d, 0, sizeof *d);
@@ -1307,4 +1257,91 @@ int mb_csr_conjugate_gradient(int32_t n, const int32_t *row_ptr, const int32_t *
     for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
     cudaStreamDestroy(s);
     return rc;
+}
+
+/* ---- internals used by the adjoint ----------------------------------------- */
+
+int mb_internal_error(int code, const char *msg) { return set_err(code, "%s", msg); }
+
+static size_t align256(size_t b) { return (b + 255u) & ~(size_t)255u; }
+
+/* snapshot layout: V | V* | FP64 state rows | FP32 state rows | control block */
+static void snapshot_layout(const mb_monodomain *m, size_t off[5], size_t len[5]) {
+    int n64, n32;
+    ode_rows(m->desc.model, m->desc.precision, &n64, &n32);
+    len[0] = (size_t)m->n * sizeof(double);
+    len[1] = (size_t)m->n * sizeof(double);
+    len[2] = (size_t)n64 * m->ode.ld * sizeof(double);
+    len[3] = (size_t)n32 * m->ode.ld * sizeof(float);
+    len[4] = sizeof(mb_ctrl);
+    size_t o = 0;
+    for (int q = 0; q < 5; ++q) {
+        off[q] = o;
+        o += align256(len[q]);
+    }
+}
+
+size_t mb_tissue_snapshot_bytes(const mb_monodomain *m) {
+    size_t off[5], len[5];
+    snapshot_layout(m, off, len);
+    return off[4] + align256(len[4]);
+}
+
+int mb_tissue_snapshot(mb_monodomain *m, void *dev, int restore) {
+    size_t off[5], len[5];
+    snapshot_layout(m, off, len);
+    void *live[5] = {m->d_v, m->d_vstar, m->d_sv64, m->d_sv32, m->d_ctrl};
+    for (int q = 0; q < 5; ++q) {
+        if (!len[q] || !live[q]) continue;
+        char *snap = (char *)dev + off[q];
+        cudaError_t e = restore ? cudaMemcpyAsync(live[q], snap, len[q], cudaMemcpyDeviceToDevice, m->stream)
+                                : cudaMemcpyAsync(snap, live[q], len[q], cudaMemcpyDeviceToDevice, m->stream);
+        if (e != cudaSuccess) return set_err(MB_ERR_CUDA, "snapshot copy: %s", cudaGetErrorString(e));
+    }
+    return MB_OK;
+}
+
+void mb_tissue_snapshot_parts(const mb_monodomain *m, void *dev, double **v, double **sv64, mb_ctrl **ctrl) {
+    size_t off[5], len[5];
+    snapshot_layout(m, off, len);
+    if (v) *v = (double *)((char *)dev + off[0]);
+    if (sv64) *sv64 = (double *)((char *)dev + off[2]);
+    if (ctrl) *ctrl = (mb_ctrl *)((char *)dev + off[4]);
+}
+
+int mb_tissue_set_sigma(mb_monodomain *m, const double *sigma_cell) {
+    if (!m || !sigma_cell || m->desc.assembly != MB_ASSEMBLY_PER_CELL_SIGMA || !m->d_fx)
+        return set_err(MB_ERR_ARG, "new conductivities need a per-cell-sigma tissue");
+    mb_monodomain_desc d = m->desc;
+    d.sigma_cell = sigma_cell;
+    mb_assembly_out a;
+    int rc = mb_assemble(&d, &a);
+    if (rc) { mb_assembly_free(&a); return set_err(rc, "assembly failed"); }
+    const size_t bytes = (size_t)m->n * sizeof(double);
+    cudaError_t e = cudaMemcpyAsync(m->d_fx, a.fx, bytes, cudaMemcpyHostToDevice, m->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->d_fy, a.fy, bytes, cudaMemcpyHostToDevice, m->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->d_fz, a.fz, bytes, cudaMemcpyHostToDevice, m->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+    mb_assembly_free(&a);
+    if (e != cudaSuccess) return set_err(MB_ERR_CUDA, "%s", cudaGetErrorString(e));
+    if (m->use_pcg) CKK(mbk_inv_diag(&m->st, m->d_invd, m->d_invd32, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return MB_OK;
+}
+
+int mb_tissue_set_scale(mb_monodomain *m, const double *scale) {
+    if (!m || !scale || !m->d_scale) return set_err(MB_ERR_ARG, "new scalings need a tissue created with scalings");
+    const size_t ld = m->ode.ld;
+    float *h = (float *)calloc((size_t)MB_NUM_SCALES * ld, sizeof(float));
+    if (!h) return set_err(MB_ERR_NOMEM, "host memory");
+    uint32_t t = 0;
+    for (int64_t g = 0; g < m->n; ++g) {
+        if (m->h_mask && !m->h_mask[g]) continue;
+        for (int q = 0; q < MB_NUM_SCALES; ++q) h[(size_t)q * ld + t] = (float)scale[(size_t)q * m->n + g];
+        ++t;
+    }
+    cudaError_t e = cudaMemcpy(m->d_scale, h, (size_t)MB_NUM_SCALES * ld * sizeof(float), cudaMemcpyHostToDevice);
+    free(h);
+    if (e != cudaSuccess) return set_err(MB_ERR_CUDA, "%s", cudaGetErrorString(e));
+    return MB_OK;
 }
