@@ -148,4 +148,33 @@ def config2_workload(scale: float = 1.0) -> Workload:
                     note=f"{len(sizes)} tissues in a {W}x{H} atlas")
 
 
+def gaussian_random_field(nx: int, ny: int, corr_cells: float, seed: int = SEED_FIELD) -> np.ndarray:
+    """Unit-variance Gaussian random field with Gaussian covariance of
+    correlation length corr_cells (in cells), made by filtering white noise
+    in Fourier space (periodic), (ny, nx)."""
+    w = rng(seed).standard_normal((ny, nx))
+    kx = np.fft.fftfreq(nx)[None, :]
+    ky = np.fft.fftfreq(ny)[:, None]
+    # covariance exp(-r^2 / (2 l^2))  <->  spectral density ~ exp(-2 pi^2 l^2 k^2)
+    filt = np.exp(-np.pi ** 2 * corr_cells ** 2 * (kx ** 2 + ky ** 2))
+    f = np.real(np.fft.ifft2(np.fft.fft2(w) * filt))
+    return (f - f.mean()) / f.std()
+
+
+def config3(scale: float = 1.0):
+    """Differentiation: 256 x 256 sheet at 100 um, TT2006, log sigma =
+    log(0.13 S/m) + 0.3 g with g a Gaussian random field of correlation
+    length 2 mm (20 cells); 64 sensor cells; V sampled every 1 ms over 200 ms;
+    gradients at uniform sigma and gKr scaling 1, checkpoints every 50 steps.
+    Returns a dict of the problem."""
+    nx = ny = max(8, int(256 * scale))
+    n = nx * ny
+    g = gaussian_random_field(nx, ny, 20.0 * scale)
+    sigma_true = 0.13 * S_PER_M * np.exp(0.3 * g.reshape(-1))
+    sensors = rng(SEED_SENSORS).choice(n, size=64, replace=False)
+    return dict(nx=nx, ny=ny, nsteps=int(round(200.0 / 0.02)), sample_every=50, checkpoint_every=50,
+                sigma_true=sigma_true, sigma0=np.full(n, 0.13 * S_PER_M), gkr0=np.ones(n), sensors=sensors,
+                stims=[Stim(kind="x_less_than", start=0.0, duration=2.0, current=-53.0, x_limit=100.0)])
+
+
 CONFIGS = {0: config0, 1: config1, 2: config2_workload, 4: config4}
