@@ -102,7 +102,7 @@ __device__ __forceinline__ bool grid_reduce(const Args &a, double (&v)[NV], doub
                     ok = 0;
                     break;
                 }
-                if (spins > 32) __nanosleep(32);
+                if (spins > 4096) __nanosleep(32);
             }
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -415,18 +415,25 @@ __device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, co
     }
 }
 
-// A pass over the groups of the block's range: act(g0, pc, ap, m) per group.
-template <typename T, int KIND, int NT, typename F, typename ACT>
+// A pass over the groups of the block's range: each thread takes U groups at
+// a time and forms all U products (their loads in flight together) before
+// act(g0, pc, ap, m) runs for each.
+template <typename T, int KIND, int NT, int U, typename F, typename ACT>
 __device__ __forceinline__ void pass4(const mb_stencil_dev &st, const F &f, ACT act) {
     const uint32_t groups = ((uint32_t)st.nx * st.ny * st.nz) >> 2;
     uint32_t c0, c1;
     block_chunk(groups, c0, c1);
-    for (uint32_t q = c0 + threadIdx.x; q < c1; q += NT) {
-        const uint32_t g0 = q << 2;
-        Vec4<T> pc, ap;
-        unsigned m[4];
-        apply4<T, KIND>(st, g0, f, pc, ap, m);
-        act(g0, pc, ap, m);
+    for (uint32_t q = c0 + threadIdx.x; q < c1; q += U * NT) {
+        Vec4<T> pc[U], ap[U];
+        unsigned m[U][4];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t qq = q + u * NT;
+            apply4<T, KIND>(st, (qq < c1 ? qq : q) << 2, f, pc[u], ap[u], m[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (q + u * NT < c1) act((q + u * NT) << 2, pc[u], ap[u], m[u]);
     }
 }
 
@@ -441,7 +448,7 @@ __device__ __forceinline__ void residual_pass(const Args &a, typename Prec<MIXED
     const mb_stencil_dev &st = a.st;
     const double *__restrict__ x = a.x;
     if constexpr (VEC) {
-        pass4<double, KIND, NT>(st, Plain<double>{x}, [&](uint32_t g0, const Vec4<double> &xc, const Vec4<double> &ax,
+        pass4<double, KIND, NT, U>(st, Plain<double>{x}, [&](uint32_t g0, const Vec4<double> &xc, const Vec4<double> &ax,
                                                         const unsigned (&m)[4]) {
             Vec4<T> rv = ld4(r, g0), pv = ld4(p, g0);
 #pragma unroll
@@ -494,10 +501,10 @@ __device__ __forceinline__ void q_pass(const Args &a, bool first, const typename
                 if (m[k] & ACTIVE) q1 += (double)pc.v[k] * (double)ap.v[k];
         };
         if (first) {
-            pass4<T, KIND, NT>(st, Plain<T>{po}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
+            pass4<T, KIND, NT, U>(st, Plain<T>{po}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
                                                      const unsigned (&m)[4]) { dot(pc, ap, m); });
         } else {
-            pass4<T, KIND, NT>(st, Direction<T>{zb, po, bt}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
+            pass4<T, KIND, NT, U>(st, Direction<T>{zb, po, bt}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
                                                                  const unsigned (&m)[4]) {
                 st4(pw, g0, pc);
                 dot(pc, ap, m);
@@ -528,7 +535,7 @@ __device__ __forceinline__ void u_pass(const Args &a, const typename Prec<MIXED>
     const T al = (T)alpha;
     double *__restrict__ x = a.x;
     if constexpr (VEC) {
-        pass4<T, KIND, NT>(st, Plain<T>{pc_}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
+        pass4<T, KIND, NT, U>(st, Plain<T>{pc_}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
                                                   const unsigned (&m)[4]) {
             Vec4<double> xv = ld4(x, g0);
             Vec4<T> rv = ld4(r, g0), zv = ld4(zb, g0);
@@ -740,9 +747,11 @@ struct Variant {
         {(const void *)k_fcg<MIXED, K, 256, 2, 4, false>, 256, 0},                                          \
         {(const void *)k_fcg<MIXED, K, 1024, 1, 1, true>, 1024, 1},                                         \
         {(const void *)k_fcg<MIXED, K, 512, 1, 2, true>, 512, 1},                                           \
-        {(const void *)k_fcg<MIXED, K, 256, 1, 4, true>, 256, 1}
+        {(const void *)k_fcg<MIXED, K, 256, 1, 4, true>, 256, 1},                                           \
+        {(const void *)k_fcg<MIXED, K, 512, 2, 1, true>, 512, 1},                                           \
+        {(const void *)k_fcg<MIXED, K, 256, 2, 2, true>, 256, 1}
 
-constexpr int NUM_VARIANTS = 8;
+constexpr int NUM_VARIANTS = 10;
 
 template <bool MIXED>
 static Variant variant_of(int kind, int v) {

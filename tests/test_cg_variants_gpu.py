@@ -42,14 +42,14 @@ def test_every_launch_shape_matches_oracle(case):
     ref = o.v()
     o.close()
     ok = np.isfinite(ref)
-    nv = 9                                       # 8 flat shapes + the tiled kernel
+    nv = 11                                      # 10 flat shapes + the tiled kernel
     old = os.environ.get("MB_CG_VARIANT")
     try:
         for v in range(nv):
             os.environ["MB_CG_VARIANT"] = str(v)
             t = Tissue(nx, ny, nz, precision="fp64", stims=stims, **kw)
             kernel = t.tuning()["cg_kernel"]
-            assert kernel == (100 if v == 8 else v), f"variant {v} not used ({kernel})"
+            assert kernel == (100 if v == nv - 1 else v), f"variant {v} not used ({kernel})"
             t.step(STEPS)
             got = t.v()
             t.close()
