@@ -87,7 +87,7 @@ __device__ __forceinline__ bool grid_reduce(const Args &a, double (&v)[NV], doub
         cuda::atomic_ref<unsigned, cuda::thread_scope_device> arrive(a.bar[0]);
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
-            double s = lane < NT / 32 ? sm[q][lane] : 0.0;
+            double s = lane < (int)(blockDim.x >> 5) ? sm[q][lane] : 0.0;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             if (lane == 0) part[(size_t)q * gridDim.x + blockIdx.x] = s;
@@ -246,16 +246,17 @@ __device__ __forceinline__ void pass(const mb_stencil_dev &st, PF pf, ACT act) {
     const uint32_t n = (uint32_t)st.nx * st.ny * st.nz;
     uint32_t c0, c1;
     block_chunk(n, c0, c1);
-    for (uint32_t base = c0 + threadIdx.x; base < c1; base += U * NT) {
+    const uint32_t nt = blockDim.x;     // <= NT: the host sizes blocks to whole rounds
+    for (uint32_t base = c0 + threadIdx.x; base < c1; base += U * nt) {
         decltype(gather<T, KIND>(st, 0u, pf)) rows[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const uint32_t g = base + u * NT;
+            const uint32_t g = base + u * nt;
             rows[u] = gather<T, KIND>(st, g < c1 ? g : base, pf);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const uint32_t g = base + u * NT;
+            const uint32_t g = base + u * nt;
             if (g < c1 && (rows[u].m & ACTIVE)) act(g, rows[u]);
         }
     }
@@ -423,17 +424,18 @@ __device__ __forceinline__ void pass4(const mb_stencil_dev &st, const F &f, ACT 
     const uint32_t groups = ((uint32_t)st.nx * st.ny * st.nz) >> 2;
     uint32_t c0, c1;
     block_chunk(groups, c0, c1);
-    for (uint32_t q = c0 + threadIdx.x; q < c1; q += U * NT) {
+    const uint32_t nt = blockDim.x;     // <= NT: the host sizes blocks to whole rounds
+    for (uint32_t q = c0 + threadIdx.x; q < c1; q += U * nt) {
         Vec4<T> pc[U], ap[U];
         unsigned m[U][4];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const uint32_t qq = q + u * NT;
+            const uint32_t qq = q + u * nt;
             apply4<T, KIND>(st, (qq < c1 ? qq : q) << 2, f, pc[u], ap[u], m[u]);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            if (q + u * NT < c1) act((q + u * NT) << 2, pc[u], ap[u], m[u]);
+            if (q + u * nt < c1) act((q + u * nt) << 2, pc[u], ap[u], m[u]);
     }
 }
 
@@ -733,23 +735,24 @@ __global__ void k_inv_diag(mb_stencil_dev st, double *d64, float *d32) {
 
 struct Variant {
     const void *fn;
-    int threads;
+    int threads;   // at most this many per block
     int groups;    // 1 = four cells per thread
+    int cells;     // units (cells or groups) each thread takes per round
 };
 
 // (threads per block, cells per thread per round, resident blocks per SM,
 // four-cell groups); the group variants need nx to be a multiple of 4
 #define MB_VARIANTS(K)                                                                                          \
-    {(const void *)k_fcg<MIXED, K, 1024, 1, 1, false>, 1024, 0},                                            \
-        {(const void *)k_fcg<MIXED, K, 1024, 1, 2, false>, 1024, 0},                                        \
-        {(const void *)k_fcg<MIXED, K, 512, 2, 2, false>, 512, 0},                                          \
-        {(const void *)k_fcg<MIXED, K, 512, 1, 4, false>, 512, 0},                                          \
-        {(const void *)k_fcg<MIXED, K, 256, 2, 4, false>, 256, 0},                                          \
-        {(const void *)k_fcg<MIXED, K, 1024, 1, 1, true>, 1024, 1},                                         \
-        {(const void *)k_fcg<MIXED, K, 512, 1, 2, true>, 512, 1},                                           \
-        {(const void *)k_fcg<MIXED, K, 256, 1, 4, true>, 256, 1},                                           \
-        {(const void *)k_fcg<MIXED, K, 512, 2, 1, true>, 512, 1},                                           \
-        {(const void *)k_fcg<MIXED, K, 256, 2, 2, true>, 256, 1}
+    {(const void *)k_fcg<MIXED, K, 1024, 1, 1, false>, 1024, 0, 1},                                         \
+        {(const void *)k_fcg<MIXED, K, 1024, 1, 2, false>, 1024, 0, 1},                                     \
+        {(const void *)k_fcg<MIXED, K, 512, 2, 2, false>, 512, 0, 2},                                       \
+        {(const void *)k_fcg<MIXED, K, 512, 1, 4, false>, 512, 0, 1},                                       \
+        {(const void *)k_fcg<MIXED, K, 256, 2, 4, false>, 256, 0, 2},                                       \
+        {(const void *)k_fcg<MIXED, K, 1024, 1, 1, true>, 1024, 1, 1},                                      \
+        {(const void *)k_fcg<MIXED, K, 512, 1, 2, true>, 512, 1, 1},                                        \
+        {(const void *)k_fcg<MIXED, K, 256, 1, 4, true>, 256, 1, 1},                                        \
+        {(const void *)k_fcg<MIXED, K, 512, 2, 1, true>, 512, 1, 2},                                        \
+        {(const void *)k_fcg<MIXED, K, 256, 2, 2, true>, 256, 1, 2}
 
 constexpr int NUM_VARIANTS = 10;
 
@@ -813,10 +816,21 @@ extern "C" int mbk_fcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
     // the arrival counter starts from zero in every launch
     cudaError_t e = cudaMemsetAsync(p->bar, 0, 2 * sizeof(unsigned), s);
     if (e != cudaSuccess) return (int)e;
+    // Block size: the fewest threads (a multiple of 32, at most the variant's)
+    // that cover each block's range in the same whole number of rounds as the
+    // variant's full block, so that no round runs partly empty.
+    const unsigned long long n = (unsigned long long)p->st.nx * p->st.ny * p->st.nz;
+    const unsigned long long units = var.groups ? n / 4 : n;
+    const unsigned long long chunk = ((units + p->blocks - 1) / p->blocks + 31) & ~31ULL;
+    const unsigned long long per_round = (unsigned long long)var.threads * var.cells;
+    const unsigned long long rounds = chunk ? (chunk + per_round - 1) / per_round : 1;
+    unsigned long long threads = ((chunk + rounds * var.cells - 1) / (rounds * var.cells) + 31) & ~31ULL;
+    if (threads < 32) threads = 32;
+    if (threads > (unsigned long long)var.threads) threads = var.threads;
     void *args[] = {&a};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(p->blocks);
-    cfg.blockDim = dim3(var.threads);
+    cfg.blockDim = dim3((unsigned)threads);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
