@@ -110,22 +110,40 @@ __device__ __forceinline__ bool grid_reduce(const Args &a, double (&v)[NV], doub
         // arrivals lane 0 observed
         cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
         if (ok) {
+            // every partial of a chunk of up to 256 blocks is loaded before any
+            // is added, so the reads cost one L2 round trip, not one per value
+            double s[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) s[q] = 0.0;
+            for (unsigned base = 0; base < gridDim.x; base += 256) {
+                double vals[NV][8];
+#pragma unroll
+                for (int q = 0; q < NV; ++q)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const unsigned bk = base + lane + 32 * j;
+                        vals[q][j] = bk < gridDim.x ? __ldcg(&part[(size_t)q * gridDim.x + bk]) : 0.0;
+                    }
+#pragma unroll
+                for (int q = 0; q < NV; ++q)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) s[q] += vals[q][j];
+            }
 #pragma unroll
             for (int q = 0; q < NV; ++q) {
-                double s = 0.0;
-                for (unsigned bk = lane; bk < gridDim.x; bk += 32) s += __ldcg(&part[(size_t)q * gridDim.x + bk]);
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0) tot[q] = s;
+                for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+                if (lane == 0) tot[q] = s[q];
             }
         }
         if (lane == 0) flag = ok;
     }
     __syncthreads();
     if (!flag) return false;
+    // tot, sm and flag are next written only after the next reduction's first
+    // __syncthreads, which every thread reaches after reading them here
 #pragma unroll
     for (int q = 0; q < NV; ++q) out[q] = tot[q];
-    __syncthreads();
     return true;
 }
 
