@@ -298,7 +298,7 @@ int mb_monodomain_time_steps_host(mb_monodomain *m, int n, const double *stim_ho
                                   double *ms);
 
 /* Launch choices made at creation by timing: the ODE kernel's register-budget
- * variant (0..3 = at least 1..4 resident 128-thread blocks per SM), the CG
+ * variant (0..5 = at least 1..6 resident 128-thread blocks per SM), the CG
  * grid size and the CG kernel (-1 = graph of separate kernels, 0.. = launch
  * shape of the persistent kernel, 100 = the 2.5D tiled persistent kernel). */
 int mb_monodomain_tuning(mb_monodomain *m, int *ode_variant, int *cg_blocks, int *cg_kernel);

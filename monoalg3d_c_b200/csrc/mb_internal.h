@@ -109,7 +109,7 @@ typedef struct mb_ode_dev {
 #define MB_ACT_STATE 6        /* 2 x activations + (1 while depolarised)    */
 #define MB_ACT_ROWS 7
 
-#define MB_ODE_VARIANTS 4     /* min resident blocks of 128 threads: 1, 2, 3, 4 */
+#define MB_ODE_VARIANTS 6     /* min resident blocks of 128 threads: 1 .. 6 */
 int mbk_ode_step_mixed(const mb_ode_dev *o, mb_ctrl *ctrl, const double *vin, double *vout,
                        cudaStream_t s);
 

@@ -279,7 +279,9 @@ k_torord_mixed(mb_ode_dev o, const mb_ctrl *__restrict__ ctrl, const double *__r
     case 0: LAUNCH(1); break;              \
     case 1: LAUNCH(2); break;              \
     case 2: LAUNCH(3); break;              \
-    default: LAUNCH(4); break;             \
+    case 3: LAUNCH(4); break;              \
+    case 4: LAUNCH(5); break;              \
+    default: LAUNCH(6); break;             \
     }
 
 MB_NS_END
