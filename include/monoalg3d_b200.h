@@ -284,6 +284,19 @@ int mb_adjoint_forward(mb_adjoint *a, const double *sigma_cell, const double *sc
 int mb_adjoint_backward(mb_adjoint *a, const double *dtraces, double *grad_sigma, double *grad_scale_gkr);
 void mb_adjoint_destroy(mb_adjoint *a);
 
+/* Checkpoint / restore of the loop state (V, V*, the ODE state rows, the
+ * clock and stimulus table, activation tracking) to host memory in this
+ * library's own layout, for a tissue of the same shape, model and precision.
+ * (The reference's save_simulation_state files, save_state.c:16-150, are not
+ * read or written.)                                                          */
+int mb_monodomain_checkpoint_bytes(mb_monodomain *m, size_t *bytes);
+int mb_monodomain_checkpoint(mb_monodomain *m, void *host, size_t bytes);
+int mb_monodomain_restore(mb_monodomain *m, const void *host, size_t bytes);
+/* V of the active cells in the format of save_as_text_or_binary
+ * (save_mesh.c:248-420): "x,y,z,hx,hy,hz,V" per line, or 7 doubles per cell
+ * when binary; cells in grid order.                                          */
+int mb_monodomain_save_v(mb_monodomain *m, const char *path, int binary);
+
 /* Device pointers to V (double, grid order) and to the CUDA stream used. */
 int mb_monodomain_device_v(mb_monodomain *m, double **v_dev, void **stream);
 /* Average duration of the last kernel launches per kind, from CUDA events

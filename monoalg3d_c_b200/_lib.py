@@ -44,7 +44,8 @@ EXPORTED = [
     "mb_monodomain_step", "mb_monodomain_sync", "mb_solve_all_volumes_odes",
     "mb_update_monodomain_default", "mb_conjugate_gradient", "mb_advance_time",
     "mb_monodomain_step_host", "mb_monodomain_get_v", "mb_monodomain_set_v", "mb_monodomain_get_activation",
-    "mb_batch_pack", "mb_adjoint_create", "mb_adjoint_forward", "mb_adjoint_backward", "mb_adjoint_destroy",
+    "mb_batch_pack", "mb_monodomain_checkpoint_bytes", "mb_monodomain_checkpoint", "mb_monodomain_restore",
+    "mb_monodomain_save_v", "mb_adjoint_create", "mb_adjoint_forward", "mb_adjoint_backward", "mb_adjoint_destroy",
     "mb_monodomain_get_state", "mb_monodomain_info", "mb_monodomain_step_stats",
     "mb_monodomain_device_v", "mb_monodomain_profile_steps", "mb_csr_conjugate_gradient",
     "mb_monodomain_tuning", "mb_monodomain_time_steps", "mb_monodomain_time_steps_host",
@@ -138,6 +139,10 @@ def _load() -> C.CDLL:
         "mb_monodomain_get_v": (i32, [vp, vp]),
         "mb_monodomain_get_activation": (i32, [vp, vp, vp, vp, vp]),
         "mb_batch_pack": (i32, [i32, vp, vp, P(i32), P(i32), vp, vp]),
+        "mb_monodomain_checkpoint_bytes": (i32, [vp, P(C.c_size_t)]),
+        "mb_monodomain_checkpoint": (i32, [vp, vp, C.c_size_t]),
+        "mb_monodomain_restore": (i32, [vp, vp, C.c_size_t]),
+        "mb_monodomain_save_v": (i32, [vp, C.c_char_p, i32]),
         "mb_adjoint_create": (i32, [P(vp), vp, i32, i32, i32, vp, i32]),
         "mb_adjoint_forward": (i32, [vp, vp, vp, vp]),
         "mb_adjoint_backward": (i32, [vp, vp, vp, vp]),

@@ -1345,3 +1345,97 @@ int mb_tissue_set_scale(mb_monodomain *m, const double *scale) {
     if (e != cudaSuccess) return set_err(MB_ERR_CUDA, "%s", cudaGetErrorString(e));
     return MB_OK;
 }
+
+/* ---- checkpoints and V files ------------------------------------------------- */
+
+typedef struct ckpt_header {
+    char magic[8];          /* "MBCKPT1" */
+    int32_t nx, ny, nz, model, precision, has_act;
+    uint64_t n_active, ld, snap_bytes, act_bytes;
+} ckpt_header;
+
+int mb_monodomain_checkpoint_bytes(mb_monodomain *m, size_t *bytes) {
+    if (!m || !bytes) return set_err(MB_ERR_ARG, "null");
+    const size_t act = m->d_act ? (size_t)MB_ACT_ROWS * m->ode.ld * sizeof(float) : 0;
+    *bytes = align256(sizeof(ckpt_header)) + mb_tissue_snapshot_bytes(m) + act;
+    return MB_OK;
+}
+
+static int ckpt_copy(mb_monodomain *m, char *host, int restore) {
+    size_t off[5], len[5];
+    snapshot_layout(m, off, len);
+    const size_t base = align256(sizeof(ckpt_header));
+    void *live[5] = {m->d_v, m->d_vstar, m->d_sv64, m->d_sv32, m->d_ctrl};
+    CK(cudaStreamSynchronize(m->stream));
+    for (int q = 0; q < 5; ++q) {
+        if (!len[q] || !live[q]) continue;
+        if (restore) CK(cudaMemcpy(live[q], host + base + off[q], len[q], cudaMemcpyHostToDevice));
+        else CK(cudaMemcpy(host + base + off[q], live[q], len[q], cudaMemcpyDeviceToHost));
+    }
+    if (m->d_act) {
+        const size_t abytes = (size_t)MB_ACT_ROWS * m->ode.ld * sizeof(float);
+        char *p = host + base + mb_tissue_snapshot_bytes(m);
+        if (restore) CK(cudaMemcpy(m->d_act, p, abytes, cudaMemcpyHostToDevice));
+        else CK(cudaMemcpy(p, m->d_act, abytes, cudaMemcpyDeviceToHost));
+    }
+    return MB_OK;
+}
+
+int mb_monodomain_checkpoint(mb_monodomain *m, void *host, size_t bytes) {
+    size_t need = 0;
+    int rc = mb_monodomain_checkpoint_bytes(m, &need);
+    if (rc) return rc;
+    if (!host || bytes < need) return set_err(MB_ERR_ARG, "checkpoint buffer smaller than %zu bytes", need);
+    if (m->phase != 0) return set_err(MB_ERR_STATE, "a split step is in progress");
+    ckpt_header h;
+    memset(&h, 0, sizeof h);
+    memcpy(h.magic, "MBCKPT1", 8);
+    h.nx = m->desc.nx; h.ny = m->desc.ny; h.nz = m->desc.nz;
+    h.model = m->desc.model; h.precision = m->desc.precision; h.has_act = m->d_act != NULL;
+    h.n_active = m->n_active; h.ld = m->ode.ld; h.snap_bytes = mb_tissue_snapshot_bytes(m);
+    h.act_bytes = m->d_act ? (uint64_t)MB_ACT_ROWS * m->ode.ld * sizeof(float) : 0;
+    memcpy(host, &h, sizeof h);
+    return ckpt_copy(m, (char *)host, 0);
+}
+
+int mb_monodomain_restore(mb_monodomain *m, const void *host, size_t bytes) {
+    size_t need = 0;
+    int rc = mb_monodomain_checkpoint_bytes(m, &need);
+    if (rc) return rc;
+    if (!host || bytes < need) return set_err(MB_ERR_ARG, "checkpoint buffer smaller than %zu bytes", need);
+    if (m->phase != 0) return set_err(MB_ERR_STATE, "a split step is in progress");
+    ckpt_header h;
+    memcpy(&h, host, sizeof h);
+    if (memcmp(h.magic, "MBCKPT1", 8) != 0 || h.nx != m->desc.nx || h.ny != m->desc.ny || h.nz != m->desc.nz ||
+        h.model != m->desc.model || h.precision != m->desc.precision || h.n_active != m->n_active ||
+        h.ld != m->ode.ld || h.snap_bytes != mb_tissue_snapshot_bytes(m) || h.has_act != (m->d_act != NULL))
+        return set_err(MB_ERR_ARG, "checkpoint does not belong to a tissue of this shape, model and precision");
+    return ckpt_copy(m, (char *)host, 1);
+}
+
+/* V of the active cells as save_as_text_or_binary writes it
+ * (save_mesh.c:248-420): per cell the centre, half the cell size and V,
+ * "%g,%g,%g,%g,%g,%g,%g\n" as text or 7 doubles as binary; cells in grid
+ * order (the reference writes its own traversal order; match by centre). */
+int mb_monodomain_save_v(mb_monodomain *m, const char *path, int binary) {
+    if (!m || !path) return set_err(MB_ERR_ARG, "null");
+    double *v = (double *)malloc((size_t)m->n * sizeof(double));
+    if (!v) return set_err(MB_ERR_NOMEM, "host memory");
+    int rc = mb_monodomain_get_v(m, v);
+    if (rc) { free(v); return rc; }
+    FILE *f = fopen(path, binary ? "wb" : "w");
+    if (!f) { free(v); return set_err(MB_ERR_ARG, "cannot open %s", path); }
+    const mb_monodomain_desc *d = &m->desc;
+    const double hx = d->dx / 2.0, hy = d->dy / 2.0, hz = d->dz / 2.0;
+    for (int64_t g = 0; g < m->n; ++g) {
+        if (m->h_mask && !m->h_mask[g]) continue;
+        const int64_t i = g % d->nx, j = (g / d->nx) % d->ny, k = g / ((int64_t)d->nx * d->ny);
+        const double rec[7] = {(i + 0.5) * d->dx, (j + 0.5) * d->dy, (k + 0.5) * d->dz, hx, hy, hz, v[g]};
+        if (binary) fwrite(rec, sizeof(double), 7, f);
+        else fprintf(f, "%g,%g,%g,%g,%g,%g,%g\n", rec[0], rec[1], rec[2], rec[3], rec[4], rec[5], rec[6]);
+    }
+    const int bad = ferror(f);
+    fclose(f);
+    free(v);
+    return bad ? set_err(MB_ERR_ARG, "write to %s failed", path) : MB_OK;
+}

@@ -226,6 +226,23 @@ class Tissue:
         v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
         check(lib.mb_monodomain_set_v(self._h, _ptr(v)))
 
+    def checkpoint(self) -> bytes:
+        """The loop state as bytes (mb_monodomain_checkpoint)."""
+        n = C.c_size_t()
+        check(lib.mb_monodomain_checkpoint_bytes(self._h, C.byref(n)))
+        buf = (C.c_char * n.value)()
+        check(lib.mb_monodomain_checkpoint(self._h, buf, n.value))
+        return bytes(buf)
+
+    def restore(self, state: bytes):
+        """Restores a state made by checkpoint() on a tissue of the same kind."""
+        buf = C.create_string_buffer(state, len(state))
+        check(lib.mb_monodomain_restore(self._h, buf, len(state)))
+
+    def save_v(self, path: str, binary: bool = False):
+        """V of the active cells in the reference's save_as_text_or_binary format."""
+        check(lib.mb_monodomain_save_v(self._h, path.encode(), 1 if binary else 0))
+
     def activation(self) -> dict:
         """Activation times tracked on the device (needs track_activation):
         first / last activation time and APD90 of the latest beat in ms (-1
