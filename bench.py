@@ -140,7 +140,7 @@ class ClockSampler:
 # workload (profiles/k_fcg_group_mixed_slab_200x200x50.md; the four-cell-group
 # launch shape, whose variants read and write the same data):
 # dram__bytes_read.sum + dram__bytes_write.sum.
-PROFILED_TRAFFIC = {"slab_200x200x50_torord_fibrosis20": 149.6e6}
+PROFILED_TRAFFIC = {("slab_200x200x50_torord_fibrosis20", "groups"): 149.6e6}
 
 
 def measured_hbm():
@@ -300,14 +300,16 @@ def main():
     refs = float(np.mean(st_mx["refinements"]))
     cg_b = cg_bytes("mixed", n_active, n_grid, its, refs, masked)
     od_b = ode_bytes(model, "mixed", n_active)
+    cg_kernel = t_mx_tuning["cg_kernel"]
     if prof_mx["cg_ms"] >= prof_mx["ode_ms"]:
-        name, b, dur = "k_pcg<mixed> (k_fcg, persistent Jacobi-PCG)", cg_b, prof_mx["cg_ms"]
+        form = {100: "k_tcg, 2.5D tiled", 200: "k_rcg, resident tile columns"}.get(cg_kernel, "k_fcg, flat")
+        name, b, dur = f"k_pcg<mixed> ({form} persistent Jacobi-PCG)", cg_b, prof_mx["cg_ms"]
     else:
         name, b, dur = f"k_{model}_mixed (Rush-Larsen ODE)", od_b, prof_mx["ode_ms"]
     achieved = b / (dur * 1e-3) / 1e9
     traffic = None
     if name.startswith("k_pcg"):
-        traffic = PROFILED_TRAFFIC.get(wl.name) if 5 <= t_mx_tuning["cg_kernel"] < 100 else None
+        traffic = PROFILED_TRAFFIC.get((wl.name, "groups" if 5 <= cg_kernel < 100 else cg_kernel))
     roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
             "bytes_per_launch": b,

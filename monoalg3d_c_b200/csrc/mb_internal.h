@@ -173,10 +173,16 @@ typedef struct mb_pcg_dev {
     mb_ctrl *ctrl;
     unsigned *bar;           /* 2 words, zero at start */
     int *status;             /* 0 = ok; set on a barrier timeout */
-    int tiled;               /* 1 = 2.5D tiled passes (cg_tiled.cu) */
+    int form;                /* MB_PCG_FLAT, MB_PCG_TILED or MB_PCG_RESIDENT */
     int variant;             /* launch-shape variant of cg_flat.cu */
     int tiles_x, tiles_y, zchunk, nchunks;
+    /* resident kernel (cg_resident.cu): shape, tile grid and tile size,
+     * dynamic shared memory per block */
+    int rc_shape, rc_nbx, rc_nby, rc_tw, rc_th;
+    size_t rc_smem;
+    double *rtrue;           /* resident kernel: FP64 true residual per cell */
 } mb_pcg_dev;
+enum { MB_PCG_FLAT = 0, MB_PCG_TILED = 1, MB_PCG_RESIDENT = 2 };
 int mbk_fcg_variants(int kind);
 int mbk_fcg_variant_groups(int variant);
 int mbk_fcg_max_blocks(int mixed, int kind, int variant);
@@ -184,6 +190,8 @@ int mbk_fcg_launch(const mb_pcg_dev *p, cudaStream_t s);
 int mbk_tcg_max_blocks(int mixed);
 int mbk_tcg_launch(const mb_pcg_dev *p, cudaStream_t s);
 void mbk_tcg_layout(int nx, int ny, int nz, int blocks, int *tiles_x, int *tiles_y, int *zchunk, int *nchunks);
+int mbk_rcg_plan(mb_pcg_dev *p);
+int mbk_rcg_launch(const mb_pcg_dev *p, cudaStream_t s);
 int mbk_inv_diag(const mb_stencil_dev *st, double *d64, float *d32, cudaStream_t s);
 int mbk_stencil_codes(const mb_stencil_dev *st, uint8_t *code, uint16_t *rowid, cudaStream_t s);
 

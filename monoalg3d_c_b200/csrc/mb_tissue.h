@@ -46,6 +46,7 @@ struct mb_monodomain {
     mb_pcg_dev pcg;
     double *d_pb, *d_ppart, *d_invd, *d_z;
     float *d_pb32, *d_invd32, *d_z32;
+    double *d_rtrue;             /* resident CG: FP64 true residual */
     unsigned *d_bar;
     int *d_status;
     float cg_tune_ms;     /* device time of one CG solve of the chosen kernel at tuning */

@@ -272,6 +272,7 @@ void mb_monodomain_destroy(mb_monodomain *m) {
     if (m->stream) cudaStreamSynchronize(m->stream);
     destroy_graphs(m);
     void *bufs[] = {m->d_pb, m->d_ppart, m->d_pb32, m->d_bar, m->d_status, m->d_invd, m->d_invd32, m->d_z, m->d_z32,
+                    m->d_rtrue,
                     m->d_mask, m->d_cells, m->d_v, m->d_vstar, m->d_r, m->d_p, m->d_r32, m->d_p32,
                     m->d_partials, m->d_sv64, m->d_sv32, m->d_stim_bits, m->d_celltype, m->d_scale,
                     m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_code, m->d_rowid, m->d_act,
@@ -320,18 +321,36 @@ static int stim_covers(const mb_stim *s, const double c[3], int64_t g) {
 static int build_graphs(mb_monodomain *m);
 static int ode_autotune(mb_monodomain *m);
 
+static int pcg_launch(const mb_pcg_dev *q, cudaStream_t s) {
+    switch (q->form) {
+    case MB_PCG_TILED: return mbk_tcg_launch(q, s);
+    case MB_PCG_RESIDENT: return mbk_rcg_launch(q, s);
+    default: return mbk_fcg_launch(q, s);
+    }
+}
+
 /* Picks the CG kernel: every launch-shape variant of the flat persistent
- * kernel and the 2.5D tiled one solve the tissue's first system (b = alpha V*
- * from the initial state) twice; V is restored after every trial and the
- * fastest by CUDA events is kept.  MB_CG_VARIANT=<n> (n = number of flat
- * variants selects the tiled kernel) forces a choice. */
+ * kernel, the 2.5D tiled one and, where its tiles fit, the resident one solve
+ * the tissue's first system (b = alpha V* from the initial state) twice; V is
+ * restored after every trial and the fastest by CUDA events is kept.
+ * MB_CG_VARIANT=<n> forces a choice (n = number of flat variants selects the
+ * tiled kernel, one more the resident kernel). */
 static int cg_autotune(mb_monodomain *m) {
     if (!m->use_pcg) return MB_OK;
     const int mixed = m->pcg.mixed;
     const int kind = m->st.kind;
     const int nv = mbk_fcg_variants(kind);
+    int resident = mbk_rcg_plan(&m->pcg);
+    if (resident && !m->d_rtrue) {
+        if (cudaMalloc((void **)&m->d_rtrue, (size_t)m->n * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            m->d_rtrue = NULL;
+            resident = 0;
+        }
+        m->pcg.rtrue = m->d_rtrue;
+    }
     const char *env = getenv("MB_CG_VARIANT");
-    int lo = 0, hi = nv;          /* candidates 0..nv-1 flat, nv tiled */
+    int lo = 0, hi = nv + 1;      /* candidates 0..nv-1 flat, nv tiled, nv+1 resident */
     if (env) lo = hi = atoi(env);
     double *vsave = NULL;
     if (cudaMalloc((void **)&vsave, (size_t)m->n * sizeof(double)) != cudaSuccess)
@@ -342,14 +361,18 @@ static int cg_autotune(mb_monodomain *m) {
     for (int cand = lo; cand <= hi && !rc; ++cand) {
         mb_pcg_dev q = m->pcg;
         if (cand < nv) {
-            q.tiled = 0;
+            q.form = MB_PCG_FLAT;
             q.variant = cand;
             q.blocks = mbk_fcg_max_blocks(mixed, kind, cand);
-        } else {
-            q.tiled = 1;
+        } else if (cand == nv) {
+            q.form = MB_PCG_TILED;
             const int items = q.tiles_x * q.tiles_y * q.nchunks;
             const int mb = mbk_tcg_max_blocks(mixed);
             q.blocks = items < mb ? items : mb;
+        } else {
+            if (!resident) continue;
+            q.form = MB_PCG_RESIDENT;
+            q.blocks = q.rc_nbx * q.rc_nby;
         }
         if (q.blocks <= 0) continue;
         if (cand < nv && mbk_fcg_variant_groups(cand) && (m->desc.nx % 4) != 0) continue;
@@ -357,7 +380,7 @@ static int cg_autotune(mb_monodomain *m) {
         for (int rep = 0; rep < 3 && !rc; ++rep) {
             cudaMemcpyAsync(m->d_v, vsave, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
             cudaEventRecord(m->ev[0], m->stream);
-            const int e = q.tiled ? mbk_tcg_launch(&q, m->stream) : mbk_fcg_launch(&q, m->stream);
+            const int e = pcg_launch(&q, m->stream);
             cudaEventRecord(m->ev[1], m->stream);
             if (e || cudaEventSynchronize(m->ev[1]) != cudaSuccess) {
                 rc = set_err(MB_ERR_CUDA, "CG tuning launch failed (candidate %d): %s", cand,
@@ -381,14 +404,22 @@ static int cg_autotune(mb_monodomain *m) {
     cudaMemcpy(&st, m->d_status, sizeof st, cudaMemcpyDeviceToHost);
     if (st) return set_err(MB_ERR_CUDA, "CG grid barrier timed out during tuning");
     if (bestc < nv) {
-        m->pcg.tiled = 0;
+        m->pcg.form = MB_PCG_FLAT;
         m->pcg.variant = bestc;
         m->pcg.blocks = mbk_fcg_max_blocks(mixed, kind, bestc);
-    } else {
-        m->pcg.tiled = 1;
+    } else if (bestc == nv) {
+        m->pcg.form = MB_PCG_TILED;
         const int items = m->pcg.tiles_x * m->pcg.tiles_y * m->pcg.nchunks;
         const int mb = mbk_tcg_max_blocks(mixed);
         m->pcg.blocks = items < mb ? items : mb;
+    } else {
+        m->pcg.form = MB_PCG_RESIDENT;
+        m->pcg.blocks = m->pcg.rc_nbx * m->pcg.rc_nby;
+    }
+    if (m->pcg.form != MB_PCG_RESIDENT && m->d_rtrue) {
+        cudaFree(m->d_rtrue);
+        m->d_rtrue = NULL;
+        m->pcg.rtrue = NULL;
     }
     m->cg_tune_ms = best / 2.0f;
     return MB_OK;
@@ -658,8 +689,10 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
             CKK(cudaMemset(m->d_status, 0, sizeof(int)));
             mb_pcg_dev *q = &m->pcg;
             q->mixed = d->precision == MB_PREC_MIXED;
-            q->tiled = 0;
+            q->form = MB_PCG_FLAT;
             q->variant = 0;
+            q->rc_shape = -1;
+            q->rtrue = NULL;
             q->blocks = mbk_fcg_max_blocks(mixed, m->st.kind, 0);
             q->x = m->d_v;
             q->vstar = m->d_vstar;
@@ -810,7 +843,10 @@ int mb_monodomain_tuning(mb_monodomain *m, int *ode_variant, int *cg_blocks, int
     if (!m) return set_err(MB_ERR_ARG, "null");
     if (ode_variant) *ode_variant = m->ode.variant;
     if (cg_blocks) *cg_blocks = m->use_pcg ? m->pcg.blocks : m->cg.grid_blocks;
-    if (cg_kernel) *cg_kernel = !m->use_pcg ? -1 : (m->pcg.tiled ? 100 : m->pcg.variant);
+    if (cg_kernel)
+        *cg_kernel = !m->use_pcg ? -1
+                   : m->pcg.form == MB_PCG_TILED ? 100
+                   : m->pcg.form == MB_PCG_RESIDENT ? 200 : m->pcg.variant;
     return MB_OK;
 }
 
@@ -895,7 +931,7 @@ static int build_loop_graph(mb_monodomain *m, capture_fn pre, capture_fn post, c
 static int cap_pcg_step(mb_monodomain *m, int in_body) {
     (void)in_body;
     int e = mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream);
-    if (!e) e = m->pcg.tiled ? mbk_tcg_launch(&m->pcg, m->stream) : mbk_fcg_launch(&m->pcg, m->stream);
+    if (!e) e = pcg_launch(&m->pcg, m->stream);
     if (!e) e = mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream);
     return e;
 }
@@ -940,7 +976,7 @@ static int cg_host_loop(mb_monodomain *m) {
 /* Enqueues one CG solve (initial residual from V*, then iterations). */
 static int cg_enqueue(mb_monodomain *m) {
     if (m->use_pcg) {
-        CKK(m->pcg.tiled ? mbk_tcg_launch(&m->pcg, m->stream) : mbk_fcg_launch(&m->pcg, m->stream));
+        CKK(pcg_launch(&m->pcg, m->stream));
         return MB_OK;
     }
     if (m->use_graphs) {
