@@ -18,6 +18,8 @@ struct Args {
     const double *b;
     double *r64, *pa64, *pb64, *z64;
     float *r32, *pa32, *pb32, *z32;
+    double *ap64;              // A p of the current direction (stored by Q, read by U)
+    float *ap32;
     const double *inv_diag64;  // Jacobi 1/diag per cell (FP64 form)
     const float *inv_diag32;   // Jacobi 1/diag per cell (mixed form)
     double *partials;          // 2 x 4 x gridDim.x partials

@@ -14,8 +14,9 @@
 //   Q: p_new = z + beta p_old (evaluated for the cell and, on the fly, for its
 //      stencil neighbours, so the direction update needs no pass of its own),
 //      A p_new and the partial sums of p.Ap;
-//   U: x += alpha p, r -= alpha A p (A p recomputed from p), z = r / diag and
-//      the partial sums of r.z and r.r.
+//   U: x += alpha p, r -= alpha A p (A p as Q stored it), z = r / diag and
+//      the partial sums of r.z and r.r; a streaming pass over the cells' own
+//      values.
 // p is double-buffered so Q reads p_old of neighbours while writing p_new.
 //
 // Rows are read without per-cell index arithmetic: each cell carries a code
@@ -179,6 +180,34 @@ template <bool MIXED>
 __device__ __forceinline__ typename Prec<MIXED>::T inv_d(const Args &a, uint32_t g) {
     if constexpr (MIXED) return a.inv_diag32[g];
     else return a.inv_diag64[g];
+}
+
+// Jacobi 1/diag of a cell: with constant coefficients (kind 0) it depends on
+// the code byte only and comes from the block's 64-entry table (filled by
+// fill_inv_table as k_inv_diag forms it), otherwise from the per-cell array.
+template <bool MIXED, int KIND>
+__device__ __forceinline__ typename Prec<MIXED>::T inv_of(const Args &a, const typename Prec<MIXED>::T *tab,
+                                                         uint32_t g, unsigned m) {
+    if constexpr (KIND == 0) return tab[m & 63u];
+    else return inv_d<MIXED>(a, g);
+}
+
+// Fills the block's table; a block may have as few as 32 threads (the host
+// sizes blocks to whole rounds of cells).
+template <bool MIXED>
+__device__ __forceinline__ void fill_inv_table(const mb_stencil_dev &st, typename Prec<MIXED>::T *tab) {
+    for (unsigned m = threadIdx.x; m < 64; m += blockDim.x) {
+        const double c[6] = {st.cx, st.cx, st.cy, st.cy, st.cz, st.cz};
+        double d64 = st.alpha;
+        float d32 = (float)st.alpha;
+        for (int q = 0; q < 6; ++q)
+            if ((m >> q) & 1u) {
+                d64 += c[q];
+                d32 += (float)c[q];
+            }
+        if constexpr (MIXED) tab[m] = 1.0f / d32;
+        else tab[m] = 1.0 / d64;
+    }
 }
 
 // ---- four cells per thread ----------------------------------------------------
@@ -351,7 +380,8 @@ __device__ __forceinline__ void pass4(const mb_stencil_dev &st, const F &f, ACT 
 // r.z (T products, FP64 sums), r.r of the stored r, and the FP64 r.r.
 template <bool MIXED, int KIND, int NT, int U, bool VEC>
 __device__ __forceinline__ void residual_pass(const Args &a, typename Prec<MIXED>::T *r,
-                                              typename Prec<MIXED>::T *p, bool pre, double (&acc)[3]) {
+                                              typename Prec<MIXED>::T *p, bool pre,
+                                              const typename Prec<MIXED>::T *itab, double (&acc)[3]) {
     using T = typename Prec<MIXED>::T;
     const mb_stencil_dev &st = a.st;
     const double *__restrict__ x = a.x;
@@ -366,7 +396,7 @@ __device__ __forceinline__ void residual_pass(const Args &a, typename Prec<MIXED
                 const double bb = a.b ? a.b[g] : st.alpha * a.vstar[g];
                 const double r64 = bb - ax.v[k];
                 const T rt = (T)r64;
-                const T z = pre ? inv_d<MIXED>(a, g) * rt : rt;
+                const T z = pre ? inv_of<MIXED, KIND>(a, itab, g, m[k]) * rt : rt;
                 rv.v[k] = rt;
                 pv.v[k] = z;
                 acc[0] += (double)rt * (double)z;
@@ -383,7 +413,7 @@ __device__ __forceinline__ void residual_pass(const Args &a, typename Prec<MIXED
                                       const double bb = a.b ? a.b[g] : st.alpha * a.vstar[g];
                                       const double r64 = bb - ax;
                                       const T rt = (T)r64;
-                                      const T z = pre ? inv_d<MIXED>(a, g) * rt : rt;
+                                      const T z = pre ? inv_of<MIXED, KIND>(a, itab, g, row.m) * rt : rt;
                                       r[g] = rt;
                                       p[g] = z;
                                       acc[0] += (double)rt * (double)z;
@@ -394,11 +424,11 @@ __device__ __forceinline__ void residual_pass(const Args &a, typename Prec<MIXED
 }
 
 // Q: the direction (p_new = z + beta p_old, or p itself on a restart), stored
-// when new, and the partial sum of p.Ap.
+// when new, A p stored for the U pass, and the partial sum of p.Ap.
 template <bool MIXED, int KIND, int NT, int U, bool VEC>
 __device__ __forceinline__ void q_pass(const Args &a, bool first, const typename Prec<MIXED>::T *po,
-                                       typename Prec<MIXED>::T *pw, const typename Prec<MIXED>::T *zb, double beta,
-                                       double &q1) {
+                                       typename Prec<MIXED>::T *pw, const typename Prec<MIXED>::T *zb,
+                                       typename Prec<MIXED>::T *apb, double beta, double &q1) {
     using T = typename Prec<MIXED>::T;
     const mb_stencil_dev &st = a.st;
     const T bt = (T)beta;
@@ -410,11 +440,15 @@ __device__ __forceinline__ void q_pass(const Args &a, bool first, const typename
         };
         if (first) {
             pass4<T, KIND, NT, U>(st, Plain<T>{po}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
-                                                     const unsigned (&m)[4]) { dot(pc, ap, m); });
+                                                     const unsigned (&m)[4]) {
+                st4(apb, g0, ap);
+                dot(pc, ap, m);
+            });
         } else {
             pass4<T, KIND, NT, U>(st, Direction<T>{zb, po, bt}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
                                                                  const unsigned (&m)[4]) {
                 st4(pw, g0, pc);
+                st4(apb, g0, ap);
                 dot(pc, ap, m);
             });
         }
@@ -422,63 +456,123 @@ __device__ __forceinline__ void q_pass(const Args &a, bool first, const typename
         if (first) {
             pass<T, KIND, NT, U>(st, [&](uint32_t q) { return po[q]; },
                                  [&](uint32_t g, const auto &row) {
-                                     q1 += (double)row.pc * (double)product<T, KIND>(st, row);
+                                     const T ap = product<T, KIND>(st, row);
+                                     apb[g] = ap;
+                                     q1 += (double)row.pc * (double)ap;
                                  });
         } else {
             pass<T, KIND, NT, U>(st, [&](uint32_t q) { return zb[q] + bt * po[q]; },
                                  [&](uint32_t g, const auto &row) {
                                      pw[g] = row.pc;
-                                     q1 += (double)row.pc * (double)product<T, KIND>(st, row);
+                                     const T ap = product<T, KIND>(st, row);
+                                     apb[g] = ap;
+                                     q1 += (double)row.pc * (double)ap;
                                  });
         }
     }
 }
 
-// U: x += alpha p, r -= alpha A p, z = r / diag; partial sums of r.z and r.r.
+// U: x += alpha p, r -= alpha A p (A p as the Q pass stored it), z = r / diag;
+// partial sums of r.z and r.r.  A streaming pass: every value it reads is the
+// cell's own.  z of removed cells is stored as 0 (no active cell couples to
+// them).
 template <bool MIXED, int KIND, int NT, int U, bool VEC>
-__device__ __forceinline__ void u_pass(const Args &a, const typename Prec<MIXED>::T *pc_, typename Prec<MIXED>::T *r,
-                                       typename Prec<MIXED>::T *zb, bool pre, double alpha, double (&u2)[2]) {
+__device__ __forceinline__ void u_pass(const Args &a, const typename Prec<MIXED>::T *pc_,
+                                       const typename Prec<MIXED>::T *apb, typename Prec<MIXED>::T *r,
+                                       typename Prec<MIXED>::T *zb, bool pre, const typename Prec<MIXED>::T *itab,
+                                       double alpha, double (&u2)[2]) {
     using T = typename Prec<MIXED>::T;
     const mb_stencil_dev &st = a.st;
     const T al = (T)alpha;
     double *__restrict__ x = a.x;
+    const uint32_t n = (uint32_t)st.nx * st.ny * st.nz;
+    const uint32_t nt = blockDim.x;
     if constexpr (VEC) {
-        pass4<T, KIND, NT, U>(st, Plain<T>{pc_}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
-                                                  const unsigned (&m)[4]) {
-            Vec4<double> xv = ld4(x, g0);
-            Vec4<T> rv = ld4(r, g0), zv = ld4(zb, g0);
-            Vec4<T> id;
-            if (pre) {
-                if constexpr (MIXED) id = ld4(a.inv_diag32, g0);
-                else id = ld4(a.inv_diag64, g0);
+        uint32_t c0, c1;
+        block_chunk(n >> 2, c0, c1);
+        for (uint32_t q = c0 + threadIdx.x; q < c1; q += U * nt) {
+            Vec4<T> pv[U], av[U], rv[U], id[U];
+            Vec4<double> xv[U];
+            unsigned m[U][4];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t qq = q + u * nt;
+                const uint32_t g0 = (qq < c1 ? qq : q) << 2;
+                if constexpr (KIND == 2) {
+                    m[u][0] = m[u][1] = m[u][2] = m[u][3] = ACTIVE;
+                } else {
+                    const uchar4 cd = *reinterpret_cast<const uchar4 *>(st.code + g0);
+                    m[u][0] = cd.x; m[u][1] = cd.y; m[u][2] = cd.z; m[u][3] = cd.w;
+                }
+                pv[u] = ld4(pc_, g0);
+                av[u] = ld4(apb, g0);
+                rv[u] = ld4(r, g0);
+                xv[u] = ld4(x, g0);
+                if constexpr (KIND != 0) {
+                    if (pre) {
+                        if constexpr (MIXED) id[u] = ld4(a.inv_diag32, g0);
+                        else id[u] = ld4(a.inv_diag64, g0);
+                    }
+                }
             }
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (!(m[k] & ACTIVE)) continue;
-                xv.v[k] += alpha * (double)pc.v[k];
-                const T rn = rv.v[k] - al * ap.v[k];
-                rv.v[k] = rn;
-                const T z = pre ? id.v[k] * rn : rn;
-                zv.v[k] = z;
+            for (int u = 0; u < U; ++u) {
+                if (q + u * nt >= c1) continue;
+                const uint32_t g0 = (q + u * nt) << 2;
+                Vec4<T> zv;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    zv.v[k] = T(0);
+                    if (!(m[u][k] & ACTIVE)) continue;
+                    xv[u].v[k] += alpha * (double)pv[u].v[k];
+                    const T rn = rv[u].v[k] - al * av[u].v[k];
+                    rv[u].v[k] = rn;
+                    T inv = T(1);
+                    if (pre) {
+                        if constexpr (KIND == 0) inv = itab[m[u][k] & 63u];
+                        else inv = id[u].v[k];
+                    }
+                    const T z = pre ? inv * rn : rn;
+                    zv.v[k] = z;
+                    u2[0] += (double)z * (double)rn;
+                    u2[1] += (double)rn * (double)rn;
+                }
+                st4(x, g0, xv[u]);
+                st4(r, g0, rv[u]);
+                st4(zb, g0, zv);
+            }
+        }
+    } else {
+        uint32_t c0, c1;
+        block_chunk(n, c0, c1);
+        for (uint32_t base = c0 + threadIdx.x; base < c1; base += U * nt) {
+            T pv[U], av[U], rv[U];
+            double xv[U];
+            unsigned m[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t gg = base + u * nt;
+                const uint32_t g = gg < c1 ? gg : base;
+                if constexpr (KIND == 2) m[u] = ACTIVE;
+                else m[u] = st.code[g];
+                pv[u] = pc_[g];
+                av[u] = apb[g];
+                rv[u] = r[g];
+                xv[u] = x[g];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t g = base + u * nt;
+                if (g >= c1 || !(m[u] & ACTIVE)) continue;
+                x[g] = xv[u] + alpha * (double)pv[u];
+                const T rn = rv[u] - al * av[u];
+                r[g] = rn;
+                const T z = pre ? inv_of<MIXED, KIND>(a, itab, g, m[u]) * rn : rn;
+                zb[g] = z;
                 u2[0] += (double)z * (double)rn;
                 u2[1] += (double)rn * (double)rn;
             }
-            st4(x, g0, xv);
-            st4(r, g0, rv);
-            st4(zb, g0, zv);
-        });
-    } else {
-        pass<T, KIND, NT, U>(st, [&](uint32_t q) { return pc_[q]; },
-                             [&](uint32_t g, const auto &row) {
-                                 const T ap = product<T, KIND>(st, row);
-                                 x[g] += alpha * (double)row.pc;
-                                 const T rn = r[g] - al * ap;
-                                 r[g] = rn;
-                                 const T z = pre ? inv_d<MIXED>(a, g) * rn : rn;
-                                 zb[g] = z;
-                                 u2[0] += (double)z * (double)rn;
-                                 u2[1] += (double)rn * (double)rn;
-                             });
+        }
     }
 }
 
@@ -494,10 +588,16 @@ __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
     T *__restrict__ zb = MIXED ? (T *)a.z32 : (T *)a.z64;
     T *bufa = MIXED ? (T *)a.pa32 : (T *)a.pa64;
     T *bufb = MIXED ? (T *)a.pb32 : (T *)a.pb64;
+    T *__restrict__ apb = MIXED ? (T *)a.ap32 : (T *)a.ap64;
+    __shared__ T itab[64];
+    if constexpr (KIND == 0) {
+        fill_inv_table<MIXED>(a.st, itab);
+        __syncthreads();
+    }
     int red = 0;
 
     double acc[3] = {0.0, 0.0, 0.0}, s3[3];
-    residual_pass<MIXED, KIND, NT, U, VEC>(a, r, bufa, pre, acc);
+    residual_pass<MIXED, KIND, NT, U, VEC>(a, r, bufa, pre, itab, acc);
     if (!grid_reduce<3, NT>(a, acc, s3, red)) return;
     double rz = s3[0], rr = s3[1];
     double error = s3[2], rr_ref = s3[2];
@@ -511,13 +611,13 @@ __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
         // Q: direction p_new = z + beta p_old fused with A p_new and p.Ap
         T *pcur = first ? pold : pnew;
         double q1[1] = {0.0}, s1[1];
-        q_pass<MIXED, KIND, NT, U, VEC>(a, first, pold, pnew, zb, beta, q1[0]);
+        q_pass<MIXED, KIND, NT, U, VEC>(a, first, pold, pnew, zb, apb, beta, q1[0]);
         if (!grid_reduce<1, NT>(a, q1, s1, red)) return;
         const double alpha = (pre ? rz : rr) / s1[0];
 
         // U: x += alpha p, r -= alpha A p, z = r / diag
         double u2[2] = {0.0, 0.0}, s2[2];
-        u_pass<MIXED, KIND, NT, U, VEC>(a, pcur, r, zb, pre, alpha, u2);
+        u_pass<MIXED, KIND, NT, U, VEC>(a, pcur, apb, r, zb, pre, itab, alpha, u2);
         if (!grid_reduce<2, NT>(a, u2, s2, red)) return;
         its += 1;
         pold = pcur;
@@ -537,7 +637,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
             if (s2[1] <= fmax(tol, ratio * rr_ref) || its >= max_its) {
                 // FP64 true residual replaces the FP32 recurrence; restart from it
                 double t3[3] = {0.0, 0.0, 0.0};
-                residual_pass<MIXED, KIND, NT, U, VEC>(a, r, pold, pre, t3);
+                residual_pass<MIXED, KIND, NT, U, VEC>(a, r, pold, pre, itab, t3);
                 if (!grid_reduce<3, NT>(a, t3, s3, red)) return;
                 refinements += 1;
                 error = s3[2];
@@ -716,6 +816,7 @@ extern "C" int mbk_fcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
     a.x = p->x; a.vstar = p->vstar; a.b = p->b;
     a.r64 = p->r64; a.pa64 = p->pa64; a.pb64 = p->pb64; a.z64 = p->z64;
     a.r32 = p->r32; a.pa32 = p->pa32; a.pb32 = p->pb32; a.z32 = p->z32;
+    a.ap64 = p->ap64; a.ap32 = p->ap32;
     a.inv_diag64 = p->inv_diag64; a.inv_diag32 = p->inv_diag32;
     a.partials = p->partials; a.ctrl = p->ctrl; a.bar = p->bar; a.status = p->status;
     const Variant var = variant(p->mixed, p->st.kind, p->variant);

@@ -167,6 +167,8 @@ typedef struct mb_pcg_dev {
     float *r32, *pa32, *pb32;
     double *z64;             /* preconditioned residual (flat kernel)     */
     float *z32;
+    double *ap64;            /* A p of the current direction (flat kernel) */
+    float *ap32;
     const double *inv_diag64;/* Jacobi 1/diag (FP64 form)   */
     const float *inv_diag32; /* Jacobi 1/diag (mixed form)  */
     double *partials;        /* 2 * 4 * blocks */

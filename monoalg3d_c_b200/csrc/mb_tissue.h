@@ -47,6 +47,8 @@ struct mb_monodomain {
     double *d_pb, *d_ppart, *d_invd, *d_z;
     float *d_pb32, *d_invd32, *d_z32;
     double *d_rtrue;             /* resident CG: FP64 true residual */
+    double *d_ap;                /* flat CG: A p (FP64 form) */
+    float *d_ap32;               /* flat CG: A p (mixed form) */
     unsigned *d_bar;
     int *d_status;
     float cg_tune_ms;     /* device time of one CG solve of the chosen kernel at tuning */
