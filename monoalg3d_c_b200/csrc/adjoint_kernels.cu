@@ -219,7 +219,7 @@ __global__ void k_adj_tol(const double *lam, int64_t n, double rel2, mb_ctrl *c)
         s = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (threadIdx.x == 0) c->tol = fmax(rel2 * s, 1e-300);
+        if (threadIdx.x == 0) c->tol = c->refine_floor = fmax(rel2 * s, 1e-300);
     }
 }
 

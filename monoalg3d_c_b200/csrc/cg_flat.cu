@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
                 first = false;
             }
         } else {
-            if (s2[1] <= fmax(tol, ratio * rr_ref) || its >= max_its) {
+            if (s2[1] <= fmax(c->refine_floor, ratio * rr_ref) || its >= max_its) {
                 // FP64 true residual replaces the FP32 recurrence; restart from it
                 double t3[3] = {0.0, 0.0, 0.0};
                 residual_pass<MIXED, KIND, NT, U, VEC>(a, r, pold, pre, itab, t3);

@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(CG_THREADS) k_cgm_update(CgArgs a) {
         if (threadIdx.x == 0) {
             mb_ctrl *c = a.ctrl;
             c->its += 1;
-            const double lim = fmax(c->tol, c->refine_ratio * c->rr_ref);
+            const double lim = fmax(c->refine_floor, c->refine_ratio * c->rr_ref);
             if (s[1] <= lim) {
                 c->phase = 1;                 // evaluate the FP64 residual next
             } else if (c->its >= c->max_its) {

@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(NT, 1) k_rcg(Args a, Tiles T, double *rtrue) {
         double u2[2] = {(double)u0, (double)u1}, s2[2];
         if (!grid_reduce<2, NT>(a, u2, s2, red)) return;
         its += 1;
-        if (s2[1] <= fmax(tol, ratio * rr_ref) || its >= max_its) {
+        if (s2[1] <= fmax(c->refine_floor, ratio * rr_ref) || its >= max_its) {
             // ---- refinement: r_true -= A d in FP64 (the FP64 residual of
             // x_ref + d), r = (float) r_true, restart from it.  d goes over
             // the padded box (own cells from D, the halo from the owners'

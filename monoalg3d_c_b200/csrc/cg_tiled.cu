@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_tcg(Args a) {
                 first = false;
             }
         } else {
-            if (s2[1] <= fmax(tol, ratio * rr_ref) || its >= max_its) {
+            if (s2[1] <= fmax(c->refine_floor, ratio * rr_ref) || its >= max_its) {
                 double t3[3] = {0.0, 0.0, 0.0};
                 residual_pass<MIXED>(a, smem, r, pold, pre, t3);
                 if (!grid_reduce<3>(a, t3, s3, red)) return;

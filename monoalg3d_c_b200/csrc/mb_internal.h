@@ -38,6 +38,8 @@ typedef struct mb_ctrl {
     double  error;
     double  tol;
     double  refine_ratio;
+    double  refine_floor;    /* mixed: the FP32 recurrence runs down to at
+                                least this r.r before the FP64 residual    */
     int32_t its;
     int32_t max_its;
     int32_t done;
@@ -109,7 +111,9 @@ typedef struct mb_ode_dev {
 #define MB_ACT_STATE 6        /* 2 x activations + (1 while depolarised)    */
 #define MB_ACT_ROWS 7
 
-#define MB_ODE_VARIANTS 6     /* min resident blocks of 128 threads: 1 .. 6 */
+#define MB_ODE_VARIANTS 10    /* 0..5: one launch, min resident blocks of 128
+                                 threads 1 .. 6; 6..9: staged persistent
+                                 kernels, min resident blocks 1 .. 4 */
 int mbk_ode_step_mixed(const mb_ode_dev *o, mb_ctrl *ctrl, const double *vin, double *vout,
                        cudaStream_t s);
 

@@ -318,6 +318,12 @@ static int stim_covers(const mb_stim *s, const double c[3], int64_t g) {
         }                                                                                  \
     } while (0)
 
+/* The mixed CG's FP32 recurrence runs down to MB_REFINE_MARGIN x tol before
+ * the FP64 true residual is evaluated (the stopping test itself is on the
+ * FP64 residual against tol).  MB_REFINE_MARGIN in the environment
+ * overrides it (tuning). */
+#define MB_REFINE_MARGIN 1.0
+
 static int build_graphs(mb_monodomain *m);
 static int ode_autotune(mb_monodomain *m);
 
@@ -753,9 +759,12 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         /* the FP32 recurrence is trusted down to refine_ratio x the last
          * FP64 r.r; MB_REFINE_RATIO overrides it (tuning) */
         c.refine_ratio = 1e-10;
+        c.refine_floor = MB_REFINE_MARGIN * c.tol;
         {
             const char *env = getenv("MB_REFINE_RATIO");
             if (env && atof(env) > 0.0) c.refine_ratio = atof(env);
+            env = getenv("MB_REFINE_MARGIN");
+            if (env && atof(env) > 0.0) c.refine_floor = atof(env) * c.tol;
         }
         c.act_dt = d->dt_pde;
         c.act_threshold = (float)(isnan(d->activation_threshold) ? -30.0 : d->activation_threshold);
@@ -830,7 +839,9 @@ static int ode_autotune(mb_monodomain *m) {
     int bestv = 0;
     for (int v = 0; v < MB_ODE_VARIANTS && !rc; ++v) {
         t.variant = v;
-        if (mbk_ode_step(&t, NULL, m->d_vstar, vs, m->stream)) { rc = set_err(MB_ERR_CUDA, "ODE tuning launch failed"); break; }
+        const int e = mbk_ode_step(&t, NULL, m->d_vstar, vs, m->stream);
+        if (e == (int)cudaErrorInvalidConfiguration && v >= 6) continue;   /* staged form does not fit */
+        if (e) { rc = set_err(MB_ERR_CUDA, "ODE tuning launch failed"); break; }
         cudaEventRecord(m->ev[0], m->stream);
         for (int q = 0; q < 3; ++q) mbk_ode_step(&t, NULL, m->d_vstar, vs, m->stream);
         cudaEventRecord(m->ev[1], m->stream);

@@ -87,19 +87,34 @@ extern "C" int mbk_ode_step(const mb_ode_dev *o, mb_ctrl *ctrl, const double *vi
     if (o->precision != MB_PREC_FP64) return mbk_ode_step_mixed(o, ctrl, vin, vout, s);
     const unsigned blocks = (o->n + ODE_THREADS - 1) / ODE_THREADS;
     const mb_ode_dev &a = *o;
+#define MB_STAGED(KERNEL, N64, N32)                                                       \
+    do {                                                                                  \
+        const size_t sm = staged_smem(N64, N32);                                          \
+        auto *kfn = KERNEL;                                                               \
+        const unsigned gb = staged_grid((const void *)kfn, sm, blocks);                   \
+        if (!gb) return (int)cudaErrorInvalidConfiguration;                               \
+        kfn<<<gb, ODE_THREADS, sm, s>>>(a, ctrl, vin, vout);                              \
+    } while (0)
     if (o->model == MB_MODEL_TT2006) {
 #define L(MB) k_tt2006_fp64<MB><<<blocks, ODE_THREADS, 0, s>>>(a, ctrl, vin, vout)
-        MB_VARIANT_SWITCH(o->variant, L)
+#define LS(MB) MB_STAGED(k_tt2006_fp64_s<MB>, TT_NEQ, 0)
+        MB_VARIANT_SWITCH(o->variant, L, LS)
 #undef L
+#undef LS
     } else if (o->rl_rule == MB_RL_TRUE) {
 #define L(MB) k_torord_fp64<MB_RL_TRUE, MB><<<blocks, ODE_THREADS, 0, s>>>(a, ctrl, vin, vout)
-        MB_VARIANT_SWITCH(o->variant, L)
+#define LS(MB) MB_STAGED((k_torord_fp64_s<MB_RL_TRUE, MB>), TOR_NEQ, 0)
+        MB_VARIANT_SWITCH(o->variant, L, LS)
 #undef L
+#undef LS
     } else {
 #define L(MB) k_torord_fp64<MB_RL_REFERENCE_CPU, MB><<<blocks, ODE_THREADS, 0, s>>>(a, ctrl, vin, vout)
-        MB_VARIANT_SWITCH(o->variant, L)
+#define LS(MB) MB_STAGED((k_torord_fp64_s<MB_RL_REFERENCE_CPU, MB>), TOR_NEQ, 0)
+        MB_VARIANT_SWITCH(o->variant, L, LS)
 #undef L
+#undef LS
     }
+#undef MB_STAGED
     return (int)cudaGetLastError();
 }
 
