@@ -140,7 +140,7 @@ class ClockSampler:
 # workload (profiles/k_fcg_group_mixed_slab_200x200x50.md; the four-cell-group
 # launch shape, whose variants read and write the same data):
 # dram__bytes_read.sum + dram__bytes_write.sum.
-PROFILED_TRAFFIC = {("slab_200x200x50_torord_fibrosis20", "groups"): 149.6e6}
+PROFILED_TRAFFIC = {("slab_200x200x50_torord_fibrosis20", "groups"): 177.3e6}
 
 
 def measured_hbm():
