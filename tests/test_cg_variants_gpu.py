@@ -3,7 +3,11 @@ thread, four-cell groups, 2.5D tiles) against the CPU oracle on each
 operator kind: constant coefficients with removed cells, per-cell
 conductivity, and the 27-point rows of fibres rotating through the wall.
 The shape the autotuner would pick is forced through MB_CG_VARIANT, which
-the tissue reads when it is created.  Bar: V within 1e-8 relative."""
+the tissue reads when it is created.  Bar: V within 1e-8 relative (FP64);
+for the mixed-precision solve, whose refinements interleave reductions of
+three values with the iteration's one and two, every shape (and the
+resident kernel where the operator allows it) within 2e-3 relative of the
+FP64 oracle and the same iteration counts as shape 0 within one."""
 import os
 import sys
 
@@ -55,6 +59,43 @@ def test_every_launch_shape_matches_oracle(case):
             t.close()
             err = np.abs(got[ok] - ref[ok])
             assert np.all(err <= 1e-8 * np.abs(ref[ok]) + 1e-9), f"{case} variant {v}: max |dV| {err.max():.3e}"
+    finally:
+        if old is None:
+            os.environ.pop("MB_CG_VARIANT", None)
+        else:
+            os.environ["MB_CG_VARIANT"] = old
+
+
+@pytest.mark.parametrize("case", ["masked", "per_cell", "rotating"])
+def test_every_launch_shape_mixed(case):
+    from monoalg3d_c_b200 import Stim, Tissue
+    nx, ny, nz, kw = _cases()[case]
+    stims = [Stim(kind="x_less_than", start=0.0, duration=2.0, current=-53.0, x_limit=500.0)]
+    o = oracle.Sim(nx, ny, nz, stims=stims, **kw)
+    o.step(STEPS)
+    ref = o.v()
+    o.close()
+    ok = np.isfinite(ref)
+    old = os.environ.get("MB_CG_VARIANT")
+    its0 = None
+    try:
+        for v in range(12):                       # 10 flat shapes, tiled, resident
+            os.environ["MB_CG_VARIANT"] = str(v)
+            t = Tissue(nx, ny, nz, precision="mixed", stims=stims, **kw)
+            kernel = t.tuning()["cg_kernel"]
+            if v == 11 and kernel != 200:
+                t.close()                         # the resident kernel does not apply to this operator
+                continue
+            assert kernel == {10: 100, 11: 200}.get(v, v), f"variant {v} not used ({kernel})"
+            t.step(STEPS)
+            got = t.v()
+            its = t.step_stats(0, STEPS)["its"]
+            t.close()
+            if its0 is None:
+                its0 = its
+            assert np.abs(its - its0).max() <= 1, f"{case} variant {v}: iteration counts differ from shape 0"
+            err = np.abs(got[ok] - ref[ok])
+            assert np.all(err <= 2e-3 * (np.abs(ref[ok]) + 1.0)), f"{case} variant {v}: max |dV| {err.max():.3e}"
     finally:
         if old is None:
             os.environ.pop("MB_CG_VARIANT", None)
