@@ -206,6 +206,13 @@ int mb_solve_model_odes_gpu(mb_ode *ode, double current_t, const double *stim_cu
 /* Copies the state, neq rows of num_cells doubles, to host memory. */
 int mb_ode_get_state(mb_ode *ode, double *host_state);
 int mb_ode_set_state(mb_ode *ode, const double *host_state);
+/* V alone (state 0 of every cell) from / to host memory with an element
+ * stride; stride = number_of_ode_equations reads and writes the reference's
+ * CPU state vector sv[i * neq] in place (what the orchestrator writes before
+ * solve_model_odes_cpu and update_monodomain_default reads after it,
+ * monodomain_solver.c:1051, update_monodomain.c:50).                       */
+int mb_ode_set_v(mb_ode *ode, const double *v, size_t stride);
+int mb_ode_get_v(mb_ode *ode, double *v, size_t stride);
 void mb_ode_destroy(mb_ode *ode);
 
 /* ---- monodomain tissue ------------------------------------------------- */
@@ -326,6 +333,16 @@ int mb_csr_conjugate_gradient(int32_t n, const int32_t *row_ptr, const int32_t *
                               const double *val, const double *b, double *x,
                               double tolerance, int max_iterations, int use_preconditioner,
                               uint32_t *number_of_iterations, double *error);
+
+/* The same solver with the matrix kept on the device between solves: create
+ * uploads it once, each solve copies b and x in and x out (the reference's
+ * conjugate_gradient plugin call, linear_system_solver_config.h:12-16, on a
+ * matrix assembled once).                                                  */
+typedef struct mb_csr mb_csr;
+int mb_csr_create(mb_csr **out, int32_t n, const int32_t *row_ptr, const int32_t *col, const double *val);
+int mb_csr_solve(mb_csr *a, const double *b, double *x, double tolerance, int max_iterations,
+                 int use_preconditioner, uint32_t *number_of_iterations, double *error);
+void mb_csr_destroy(mb_csr *a);
 
 /* ---- allocation-free CSR CG -------------------------------------------- */
 /* No counterpart in the reference.  The same solve as

@@ -39,7 +39,8 @@ MB_NUM_SCALES = 5
 EXPORTED = [
     "mb_last_error", "mb_version", "mb_device_count", "mb_init_cell_model_data",
     "mb_ode_create", "mb_set_model_initial_conditions_gpu", "mb_solve_model_odes_gpu",
-    "mb_ode_get_state", "mb_ode_set_state", "mb_ode_destroy",
+    "mb_ode_get_state", "mb_ode_set_state", "mb_ode_set_v", "mb_ode_get_v", "mb_ode_destroy",
+    "mb_csr_create", "mb_csr_solve", "mb_csr_destroy",
     "mb_monodomain_desc_defaults", "mb_monodomain_create", "mb_monodomain_destroy",
     "mb_monodomain_step", "mb_monodomain_sync", "mb_solve_all_volumes_odes",
     "mb_update_monodomain_default", "mb_conjugate_gradient", "mb_advance_time",
@@ -125,6 +126,8 @@ def _load() -> C.CDLL:
         "mb_solve_model_odes_gpu": (i32, [vp, dbl, vp]),
         "mb_ode_get_state": (i32, [vp, vp]),
         "mb_ode_set_state": (i32, [vp, vp]),
+        "mb_ode_set_v": (i32, [vp, vp, C.c_size_t]),
+        "mb_ode_get_v": (i32, [vp, vp, C.c_size_t]),
         "mb_ode_destroy": (None, [vp]),
         "mb_monodomain_desc_defaults": (None, [P(MbDesc)]),
         "mb_monodomain_create": (i32, [P(vp), P(MbDesc)]),
@@ -154,6 +157,9 @@ def _load() -> C.CDLL:
         "mb_monodomain_device_v": (i32, [vp, P(vp), P(vp)]),
         "mb_monodomain_profile_steps": (i32, [vp, i32, P(dbl), P(dbl), P(dbl), P(i32)]),
         "mb_csr_conjugate_gradient": (i32, [i32, vp, vp, vp, vp, vp, dbl, i32, i32, P(u32), P(dbl)]),
+        "mb_csr_create": (i32, [P(vp), i32, vp, vp, vp]),
+        "mb_csr_solve": (i32, [vp, vp, vp, dbl, i32, i32, P(u32), P(dbl)]),
+        "mb_csr_destroy": (None, [vp]),
         "mb_monodomain_tuning": (i32, [vp, P(i32), P(i32), P(i32)]),
         "mb_monodomain_time_steps": (i32, [vp, i32, P(dbl)]),
         "mb_monodomain_time_steps_host": (i32, [vp, i32, vp, vp, P(dbl)]),

@@ -228,6 +228,34 @@ int mb_ode_set_state(mb_ode *o, const double *host_state) {
     return MB_OK;
 }
 
+/* V of every cell (row 0 of the state) from / to host memory with an
+ * element stride: stride = the number of equations reads and writes the
+ * reference's array-of-structures state vector (sv[i * neq]) in place. */
+int mb_ode_set_v(mb_ode *o, const double *v, size_t stride) {
+    if (!o || !v || stride == 0) return set_err(MB_ERR_ARG, "bad arguments");
+    const size_t n = o->dev.n;
+    double *tmp = (double *)malloc(n * sizeof(double));
+    if (!tmp) return set_err(MB_ERR_NOMEM, "out of host memory");
+    for (size_t i = 0; i < n; ++i) tmp[i] = v[i * stride];
+    cudaError_t e = cudaMemcpyAsync(o->dev.sv64, tmp, n * sizeof(double), cudaMemcpyHostToDevice, o->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(o->stream);
+    free(tmp);
+    return e == cudaSuccess ? MB_OK : set_err(MB_ERR_CUDA, "mb_ode_set_v: %s", cudaGetErrorString(e));
+}
+
+int mb_ode_get_v(mb_ode *o, double *v, size_t stride) {
+    if (!o || !v || stride == 0) return set_err(MB_ERR_ARG, "bad arguments");
+    const size_t n = o->dev.n;
+    double *tmp = (double *)malloc(n * sizeof(double));
+    if (!tmp) return set_err(MB_ERR_NOMEM, "out of host memory");
+    cudaError_t e = cudaMemcpyAsync(tmp, o->dev.sv64, n * sizeof(double), cudaMemcpyDeviceToHost, o->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(o->stream);
+    if (e == cudaSuccess)
+        for (size_t i = 0; i < n; ++i) v[i * stride] = tmp[i];
+    free(tmp);
+    return e == cudaSuccess ? MB_OK : set_err(MB_ERR_CUDA, "mb_ode_get_v: %s", cudaGetErrorString(e));
+}
+
 /* ---- monodomain tissue --------------------------------------------------- */
 
 /* struct mb_monodomain: mb_tissue.h */
@@ -1249,65 +1277,101 @@ int mb_monodomain_profile_steps(mb_monodomain *m, int n, double *ode_ms, double 
 
 /* ---- general CSR CG -------------------------------------------------------- */
 
-int mb_csr_conjugate_gradient(int32_t n, const int32_t *row_ptr, const int32_t *col, const double *val,
-                              const double *b, double *x, double tolerance, int max_iterations,
-                              int use_preconditioner, uint32_t *number_of_iterations, double *error) {
-    if (n <= 0 || !row_ptr || !col || !val || !b || !x) return set_err(MB_ERR_ARG, "bad arguments");
-    const int32_t nnz = row_ptr[n];
+/* A CSR system kept on the device between solves (the reference-host shim
+ * uploads the assembled matrix once and solves every step). */
+struct mb_csr {
     mb_csr_dev a;
-    memset(&a, 0, sizeof a);
-    a.n = n;
+    int32_t *d_rp, *d_col;
+    double *d_val, *d_b, *d_x, *d_r, *d_p, *d_q, *d_id, *d_part;
+    mb_ctrl *d_ctrl;
+    cudaStream_t s;
+};
+
+void mb_csr_destroy(mb_csr *m) {
+    if (!m) return;
+    if (m->s) cudaStreamSynchronize(m->s);
+    void *bufs[] = {m->d_rp, m->d_col, m->d_val, m->d_b, m->d_x, m->d_r, m->d_p, m->d_q, m->d_id, m->d_part, m->d_ctrl};
+    for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
+    if (m->s) cudaStreamDestroy(m->s);
+    free(m);
+}
+
+int mb_csr_create(mb_csr **out, int32_t n, const int32_t *row_ptr, const int32_t *col, const double *val) {
+    if (!out || n <= 0 || !row_ptr || !col || !val) return set_err(MB_ERR_ARG, "bad arguments");
+    const int32_t nnz = row_ptr[n];
+    if (nnz < 0) return set_err(MB_ERR_ARG, "bad row_ptr");
+    mb_csr *m = (mb_csr *)calloc(1, sizeof *m);
+    if (!m) return set_err(MB_ERR_NOMEM, "out of host memory");
     int gb = (n + 255) / 256;
     if (gb > mbk_max_grid_blocks()) gb = mbk_max_grid_blocks();
-    a.grid_blocks = gb;
-    int32_t *d_rp = NULL, *d_col = NULL;
-    double *d_val = NULL, *d_b = NULL, *d_x = NULL, *d_r = NULL, *d_p = NULL, *d_q = NULL, *d_id = NULL, *d_part = NULL;
-    mb_ctrl *d_ctrl = NULL;
-    cudaStream_t s = NULL;
-    int rc = MB_OK;
-    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    CK(cudaMalloc((void **)&d_rp, (size_t)(n + 1) * sizeof(int32_t)));
-    CK(cudaMalloc((void **)&d_col, (size_t)nnz * sizeof(int32_t)));
-    CK(cudaMalloc((void **)&d_val, (size_t)nnz * sizeof(double)));
-    CK(cudaMalloc((void **)&d_b, (size_t)n * sizeof(double)));
-    CK(cudaMalloc((void **)&d_x, (size_t)n * sizeof(double)));
-    CK(cudaMalloc((void **)&d_r, (size_t)n * sizeof(double)));
-    CK(cudaMalloc((void **)&d_p, (size_t)n * sizeof(double)));
-    CK(cudaMalloc((void **)&d_q, (size_t)n * sizeof(double)));
-    CK(cudaMalloc((void **)&d_id, (size_t)n * sizeof(double)));
-    CK(cudaMalloc((void **)&d_part, (size_t)3 * gb * sizeof(double)));
-    CK(cudaMalloc((void **)&d_ctrl, sizeof(mb_ctrl)));
-    CK(cudaMemcpy(d_rp, row_ptr, (size_t)(n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_col, col, (size_t)nnz * sizeof(int32_t), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_val, val, (size_t)nnz * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_b, b, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_x, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    cudaError_t e = cudaStreamCreateWithFlags(&m->s, cudaStreamNonBlocking);
+#define CSR_ALLOC(p, bytes) if (e == cudaSuccess) e = cudaMalloc((void **)&(p), (bytes))
+    CSR_ALLOC(m->d_rp, (size_t)(n + 1) * sizeof(int32_t));
+    CSR_ALLOC(m->d_col, (size_t)(nnz ? nnz : 1) * sizeof(int32_t));
+    CSR_ALLOC(m->d_val, (size_t)(nnz ? nnz : 1) * sizeof(double));
+    CSR_ALLOC(m->d_b, (size_t)n * sizeof(double));
+    CSR_ALLOC(m->d_x, (size_t)n * sizeof(double));
+    CSR_ALLOC(m->d_r, (size_t)n * sizeof(double));
+    CSR_ALLOC(m->d_p, (size_t)n * sizeof(double));
+    CSR_ALLOC(m->d_q, (size_t)n * sizeof(double));
+    CSR_ALLOC(m->d_id, (size_t)n * sizeof(double));
+    CSR_ALLOC(m->d_part, (size_t)3 * gb * sizeof(double));
+    CSR_ALLOC(m->d_ctrl, sizeof(mb_ctrl));
+#undef CSR_ALLOC
+    if (e == cudaSuccess) e = cudaMemcpy(m->d_rp, row_ptr, (size_t)(n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nnz) e = cudaMemcpy(m->d_col, col, (size_t)nnz * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nnz) e = cudaMemcpy(m->d_val, val, (size_t)nnz * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        mb_csr_destroy(m);
+        return set_err(MB_ERR_CUDA, "mb_csr_create: %s", cudaGetErrorString(e));
+    }
+    mb_csr_dev *a = &m->a;
+    a->n = n;
+    a->grid_blocks = gb;
+    a->row_ptr = m->d_rp; a->col = m->d_col; a->val = m->d_val; a->b = m->d_b; a->x = m->d_x;
+    a->r = m->d_r; a->p = m->d_p; a->q = m->d_q; a->inv_diag = m->d_id; a->partials = m->d_part;
+    *out = m;
+    return MB_OK;
+}
+
+int mb_csr_solve(mb_csr *m, const double *b, double *x, double tolerance, int max_iterations,
+                 int use_preconditioner, uint32_t *number_of_iterations, double *error) {
+    if (!m || !b || !x) return set_err(MB_ERR_ARG, "bad arguments");
+    const size_t bytes = (size_t)m->a.n * sizeof(double);
+    CK(cudaMemcpyAsync(m->d_b, b, bytes, cudaMemcpyHostToDevice, m->s));
+    CK(cudaMemcpyAsync(m->d_x, x, bytes, cudaMemcpyHostToDevice, m->s));
     mb_ctrl c;
     memset(&c, 0, sizeof c);
     c.tol = tolerance;
     c.max_its = max_iterations;
     c.use_precond = use_preconditioner ? 1 : 0;
-    CK(cudaMemcpy(d_ctrl, &c, sizeof c, cudaMemcpyHostToDevice));
-    a.row_ptr = d_rp; a.col = d_col; a.val = d_val; a.b = d_b; a.x = d_x; a.r = d_r; a.p = d_p; a.q = d_q;
-    a.inv_diag = d_id; a.partials = d_part;
-    if (mbk_csr_cg_init(&a, d_ctrl, s)) rc = set_err(MB_ERR_CUDA, "csr init launch failed");
-    for (int it = 0; !rc && it < max_iterations + 1; it += 16) {
-        for (int q = 0; q < 16 && !rc; ++q)
-            if (mbk_csr_cg_iter(&a, d_ctrl, s)) rc = set_err(MB_ERR_CUDA, "csr iteration launch failed");
+    CK(cudaMemcpyAsync(m->d_ctrl, &c, sizeof c, cudaMemcpyHostToDevice, m->s));
+    if (mbk_csr_cg_init(&m->a, m->d_ctrl, m->s)) return set_err(MB_ERR_CUDA, "csr init launch failed");
+    for (int it = 0; it < max_iterations + 1; it += 16) {
+        for (int q = 0; q < 16; ++q)
+            if (mbk_csr_cg_iter(&m->a, m->d_ctrl, m->s)) return set_err(MB_ERR_CUDA, "csr iteration launch failed");
         int32_t done = 0;
-        cudaMemcpyAsync(&done, &d_ctrl->done, sizeof done, cudaMemcpyDeviceToHost, s);
-        cudaStreamSynchronize(s);
+        CK(cudaMemcpyAsync(&done, &m->d_ctrl->done, sizeof done, cudaMemcpyDeviceToHost, m->s));
+        CK(cudaStreamSynchronize(m->s));
         if (done) break;
     }
-    if (!rc) {
-        cudaMemcpy(&c, d_ctrl, sizeof c, cudaMemcpyDeviceToHost);
-        cudaMemcpy(x, d_x, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
-        if (number_of_iterations) *number_of_iterations = (uint32_t)c.its;
-        if (error) *error = c.error;
-    }
-    void *bufs[] = {d_rp, d_col, d_val, d_b, d_x, d_r, d_p, d_q, d_id, d_part, d_ctrl};
-    for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
-    cudaStreamDestroy(s);
+    CK(cudaMemcpyAsync(&c, m->d_ctrl, sizeof c, cudaMemcpyDeviceToHost, m->s));
+    CK(cudaMemcpyAsync(x, m->d_x, bytes, cudaMemcpyDeviceToHost, m->s));
+    CK(cudaStreamSynchronize(m->s));
+    if (number_of_iterations) *number_of_iterations = (uint32_t)c.its;
+    if (error) *error = c.error;
+    return MB_OK;
+}
+
+int mb_csr_conjugate_gradient(int32_t n, const int32_t *row_ptr, const int32_t *col, const double *val,
+                              const double *b, double *x, double tolerance, int max_iterations,
+                              int use_preconditioner, uint32_t *number_of_iterations, double *error) {
+    if (n <= 0 || !row_ptr || !col || !val || !b || !x) return set_err(MB_ERR_ARG, "bad arguments");
+    mb_csr *m = NULL;
+    int rc = mb_csr_create(&m, n, row_ptr, col, val);
+    if (rc) return rc;
+    rc = mb_csr_solve(m, b, x, tolerance, max_iterations, use_preconditioner, number_of_iterations, error);
+    mb_csr_destroy(m);
     return rc;
 }
 

@@ -1,0 +1,68 @@
+"""Drop-in test: the unmodified reference MonoAlg3D binary (its CPU build,
+oracle/_ref, built from its own sources) runs its own time loop twice on the
+same ini, once with its stock cell-model and linear-solver plugins and once
+with this library's reference-host plugins (monoalg3d_c_b200/shim: the
+same entry points, the ODE and CG work on the GPU) named in [ode_solver]
+and [linear_system_solver] library_file.  The V dumps (the reference's own
+save_as_text_or_binary writer) and the CG iteration counts of the two runs
+are compared.  Bar: V within 1e-8 relative (FP64), identical iteration
+counts."""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import make_golden as mg  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+SHIM = {"tt2006": os.path.join(REPO, "monoalg3d_c_b200", "shim", "libmb_shim_tt2006.so"),
+        "torord": os.path.join(REPO, "monoalg3d_c_b200", "shim", "libmb_shim_torord.so")}
+MODEL_LIB = {"tt2006": "libten_tusscher_2006.so", "torord": "libToRORd_fkatp_mixed_endo_mid_epi.so"}
+
+
+def _run(case, shim):
+    with tempfile.TemporaryDirectory() as tmp:
+        out_dir = os.path.join(tmp, "out")
+        text = mg.ini_text(case, out_dir)
+        if shim:
+            lib = SHIM[case["model"]]
+            stock_model = f"library_file={mg.LIBS}/{MODEL_LIB[case['model']]}"
+            stock_solver = f"library_file={mg.LIBS}/libdefault_linear_system_solver.so"
+            assert stock_model in text and stock_solver in text
+            text = text.replace(stock_model, f"library_file={lib}").replace(stock_solver, f"library_file={lib}")
+        ini = os.path.join(tmp, "case.ini")
+        with open(ini, "w") as f:
+            f.write(text)
+        log = subprocess.run([mg.BIN, "-c", ini, "-p", "1"], capture_output=True, text=True, timeout=600)
+        assert log.returncode == 0, log.stdout[-2000:] + log.stderr[-2000:]
+        its = [int(m.group(2)) for m in mg.re.finditer(
+            r"t = ([0-9.]+), Iterations = (\d+), Error Norm = ([0-9.eE+-]+)", log.stdout)]
+        files = sorted((int(mg.re.match(r"V_it_(\d+)\.bin$", f).group(1)), f)
+                       for f in os.listdir(out_dir) if mg.re.match(r"V_it_\d+\.bin$", f))
+        V = np.stack([mg.read_bin(os.path.join(out_dir, f), case["nx"], case["ny"], case["nz"]) for _, f in files])
+        return np.array(its), V, [c for c, _ in files]
+
+
+@pytest.mark.skipif(not os.path.exists(mg.BIN), reason="the reference build (oracle/_ref) is not present")
+@pytest.mark.parametrize("name", ["tt2006_cuboid", "torord_endo_cuboid", "tt2006_aniso_30"])
+def test_reference_binary_with_shim(name):
+    case = mg.CASES[name]
+    model = case["model"]
+    if not os.path.exists(SHIM[model]):
+        pytest.skip("the shim is built only where the reference headers are mounted")
+    its_ref, v_ref, counts_ref = _run(case, shim=False)
+    its, v, counts = _run(case, shim=True)
+    assert counts == counts_ref and len(its) == len(its_ref) and len(its) > 100
+    assert np.array_equal(its, its_ref), f"{name}: CG iteration counts differ"
+    ok = np.isfinite(v_ref)
+    assert np.array_equal(ok, np.isfinite(v))
+    err = np.abs(v[ok] - v_ref[ok])
+    print(f"{name}: {len(its)} steps, max |dV| {err.max():.3e} mV")
+    assert np.all(err <= 1e-8 * np.abs(v_ref[ok]) + 1e-9), f"{name}: max |dV| {err.max():.3e} mV"
