@@ -168,7 +168,20 @@ typedef struct mb_monodomain_desc {
     int    track_activation;
     double activation_threshold;       /* mV, default -30                     */
     double activation_min_interval;    /* ms, default 10                      */
+    /* [calc_ecg] pseudo_bidomain (ecg_library/ecg.c:204-307): at the start
+       of every step whose count is a multiple of ecg_rate, from the V of
+       that moment; 0 = off.  Electrodes at ecg_leads (3 per lead, um, in
+       the grid's frame: cell (i,j,k) is centred at ((i+1/2)dx, ...)), at
+       most MB_ECG_MAX_LEADS; records kept on the device, at most
+       ecg_capacity (read with mb_monodomain_get_ecg).                      */
+    int    ecg_rate;
+    int    ecg_n_leads;
+    const double *ecg_leads;
+    double ecg_sigma_b;                /* bath conductivity, sigma_b of the reference */
+    int64_t ecg_capacity;
 } mb_monodomain_desc;
+
+#define MB_ECG_MAX_LEADS 16
 
 /* Scalings of the ionic conductances, in this order (TT2006: gNa, gKr, gKs,
  * gCaL, gK1; ToRORd: the same currents).                                    */
@@ -257,6 +270,14 @@ int mb_monodomain_step_stats(mb_monodomain *m, int64_t first, int64_t n, mb_step
  * activated, beats not yet repolarised and removed cells read -1 (count 0).
  * Any pointer may be NULL.                                                  */
 int mb_monodomain_get_activation(mb_monodomain *m, float *first, float *last, float *apd90, int32_t *count);
+
+/* ECG records taken so far (*records), and records first .. first+n-1 of
+ * them: times[n] (ms, the loop clock of the step) and values[n x n_leads]
+ * (lead after lead, the reference's ecg.txt columns: -1/(4 pi sigma_b)
+ * sum over active cells of beta_im vol / |x - lead|, ecg.c:264-307).
+ * Either array may be NULL.                                                */
+int mb_monodomain_get_ecg(mb_monodomain *m, int64_t first, int64_t n, double *times, double *values,
+                          int64_t *records);
 
 /* ---- batches of independent tissues ------------------------------------
  * No counterpart in the reference (which runs one tissue per process).  The

@@ -45,6 +45,7 @@ EXPORTED = [
     "mb_monodomain_step", "mb_monodomain_sync", "mb_solve_all_volumes_odes",
     "mb_update_monodomain_default", "mb_conjugate_gradient", "mb_advance_time",
     "mb_monodomain_step_host", "mb_monodomain_get_v", "mb_monodomain_set_v", "mb_monodomain_get_activation",
+    "mb_monodomain_get_ecg",
     "mb_batch_pack", "mb_monodomain_checkpoint_bytes", "mb_monodomain_checkpoint", "mb_monodomain_restore",
     "mb_monodomain_save_v", "mb_adjoint_create", "mb_adjoint_forward", "mb_adjoint_backward", "mb_adjoint_destroy",
     "mb_monodomain_get_state", "mb_monodomain_info", "mb_monodomain_step_stats",
@@ -93,6 +94,11 @@ class MbDesc(C.Structure):
         ("track_activation", C.c_int),
         ("activation_threshold", C.c_double),
         ("activation_min_interval", C.c_double),
+        ("ecg_rate", C.c_int),
+        ("ecg_n_leads", C.c_int),
+        ("ecg_leads", C.c_void_p),
+        ("ecg_sigma_b", C.c_double),
+        ("ecg_capacity", C.c_int64),
     ]
 
 
@@ -141,6 +147,7 @@ def _load() -> C.CDLL:
         "mb_monodomain_step_host": (i32, [vp, vp, vp]),
         "mb_monodomain_get_v": (i32, [vp, vp]),
         "mb_monodomain_get_activation": (i32, [vp, vp, vp, vp, vp]),
+        "mb_monodomain_get_ecg": (i32, [vp, i64, i64, vp, vp, P(i64)]),
         "mb_batch_pack": (i32, [i32, vp, vp, P(i32), P(i32), vp, vp]),
         "mb_monodomain_checkpoint_bytes": (i32, [vp, P(C.c_size_t)]),
         "mb_monodomain_checkpoint": (i32, [vp, vp, C.c_size_t]),

@@ -52,6 +52,8 @@ typedef struct mb_ctrl {
     double  act_dt;          /* loop step dt_pde                            */
     float   act_threshold;   /* upward crossing that marks an activation    */
     float   act_min_interval;/* ms between two counted activations          */
+    /* pseudo-bidomain ECG */
+    int64_t ecg_count;       /* records written                              */
 } mb_ctrl;
 
 /* Structured grid, device view. */
@@ -199,6 +201,18 @@ void mbk_tcg_layout(int nx, int ny, int nz, int blocks, int *tiles_x, int *tiles
 int mbk_rcg_plan(mb_pcg_dev *p);
 int mbk_rcg_launch(const mb_pcg_dev *p, cudaStream_t s);
 int mbk_inv_diag(const mb_stencil_dev *st, double *d64, float *d32, cudaStream_t s);
+
+/* Pseudo-bidomain ECG at the start of a step (ecg.cu). */
+typedef struct mb_ecg_dev {
+    int32_t rate, n_leads;
+    int64_t capacity;
+    double dx, dy, dz, scale;  /* scale = 1 / (4 pi sigma_b) */
+    const double *leads;       /* 3 x n_leads */
+    double *partials;          /* MB_ECG_BLOCKS x MB_ECG_MAX_LEADS */
+    double *log;               /* capacity x (1 + n_leads): time, leads */
+} mb_ecg_dev;
+#define MB_ECG_BLOCKS 296
+int mbk_ecg(const mb_stencil_dev *st, const double *v, const mb_ecg_dev *e, mb_ctrl *ctrl, cudaStream_t s);
 int mbk_stencil_codes(const mb_stencil_dev *st, uint8_t *code, uint16_t *rowid, cudaStream_t s);
 
 #ifdef __cplusplus

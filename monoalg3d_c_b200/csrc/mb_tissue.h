@@ -36,6 +36,9 @@ struct mb_monodomain {
     uint8_t *d_code;      /* per-cell coupling codes (kinds 0, 1) */
     uint16_t *d_rowid;    /* per-cell class-table rows (kind 2)   */
     float *d_act;         /* activation tracking rows, or NULL    */
+    int use_ecg;          /* pseudo-bidomain ECG records at step starts */
+    mb_ecg_dev ecg;
+    double *d_ecg_leads, *d_ecg_part, *d_ecg_log;
     double *d_stim_host;
     mb_ctrl *d_ctrl;
     mb_step_stats *d_log;

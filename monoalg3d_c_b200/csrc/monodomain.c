@@ -300,7 +300,7 @@ void mb_monodomain_destroy(mb_monodomain *m) {
     if (m->stream) cudaStreamSynchronize(m->stream);
     destroy_graphs(m);
     void *bufs[] = {m->d_pb, m->d_ppart, m->d_pb32, m->d_bar, m->d_status, m->d_invd, m->d_invd32, m->d_z, m->d_z32,
-                    m->d_rtrue, m->d_ap, m->d_ap32,
+                    m->d_rtrue, m->d_ap, m->d_ap32, m->d_ecg_leads, m->d_ecg_part, m->d_ecg_log,
                     m->d_mask, m->d_cells, m->d_v, m->d_vstar, m->d_r, m->d_p, m->d_r32, m->d_p32,
                     m->d_partials, m->d_sv64, m->d_sv32, m->d_stim_bits, m->d_celltype, m->d_scale,
                     m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_code, m->d_rowid, m->d_act,
@@ -354,6 +354,16 @@ static int stim_covers(const mb_stim *s, const double c[3], int64_t g) {
 
 static int build_graphs(mb_monodomain *m);
 static int ode_autotune(mb_monodomain *m);
+
+/* The start of a loop step: the ECG record of V_n when one is due
+ * (monodomain_solver.c:654-657), then the cell models. */
+static int step_ode(mb_monodomain *m) {
+    if (m->use_ecg) {
+        const int e = mbk_ecg(&m->st, m->d_v, &m->ecg, m->d_ctrl, m->stream);
+        if (e) return e;
+    }
+    return mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream);
+}
 
 static int pcg_launch(const mb_pcg_dev *q, cudaStream_t s) {
     switch (q->form) {
@@ -747,6 +757,30 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         }
     }
 
+    /* pseudo-bidomain ECG records (ecg.cu), taken at step starts */
+    if (d->ecg_rate > 0) {
+        const int nl = d->ecg_n_leads;
+        if (nl < 1 || nl > MB_ECG_MAX_LEADS || !d->ecg_leads || d->ecg_capacity < 1 || !(d->ecg_sigma_b != 0.0)) {
+            rc = set_err(MB_ERR_ARG, "ECG: 1..%d leads, a record capacity and a nonzero sigma_b are needed",
+                         MB_ECG_MAX_LEADS);
+            goto fail;
+        }
+        ALLOC(m->d_ecg_leads, (size_t)3 * nl * sizeof(double));
+        UPLOAD(m->d_ecg_leads, d->ecg_leads, (size_t)3 * nl * sizeof(double));
+        ALLOC(m->d_ecg_part, (size_t)MB_ECG_BLOCKS * MB_ECG_MAX_LEADS * sizeof(double));
+        ALLOC(m->d_ecg_log, (size_t)d->ecg_capacity * (1 + nl) * sizeof(double));
+        mb_ecg_dev *e = &m->ecg;
+        e->rate = d->ecg_rate;
+        e->n_leads = nl;
+        e->capacity = d->ecg_capacity;
+        e->dx = d->dx; e->dy = d->dy; e->dz = d->dz;
+        e->scale = 1.0 / (4.0 * M_PI * d->ecg_sigma_b);   /* ecg.c:236 */
+        e->leads = m->d_ecg_leads;
+        e->partials = m->d_ecg_part;
+        e->log = m->d_ecg_log;
+        m->use_ecg = 1;
+    }
+
     /* activation tracking rows (read and written by the ODE kernels) */
     if (d->track_activation) {
         const size_t ld = m->ode.ld, bytes = (size_t)MB_ACT_ROWS * ld * sizeof(float);
@@ -899,7 +933,7 @@ typedef int (*capture_fn)(mb_monodomain *m, int in_body);
 
 static int cap_pre(mb_monodomain *m, int in_body) {
     (void)in_body;
-    int e = mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream);
+    int e = step_ode(m);
     if (!e) e = mbk_cg_init(&m->st, &m->cg, m->d_ctrl, 0ULL, 0, m->stream);
     return e;
 }
@@ -974,7 +1008,7 @@ static int build_loop_graph(mb_monodomain *m, capture_fn pre, capture_fn post, c
 
 static int cap_pcg_step(mb_monodomain *m, int in_body) {
     (void)in_body;
-    int e = mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream);
+    int e = step_ode(m);
     if (!e) e = pcg_launch(&m->pcg, m->stream);
     if (!e) e = mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream);
     return e;
@@ -1035,7 +1069,7 @@ static int step_once(mb_monodomain *m) {
         CK(cudaGraphLaunch(m->ge_step, m->stream));
         return MB_OK;
     }
-    CKK(mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
+    CKK(step_ode(m));
     int rc = cg_enqueue(m);
     if (rc) return rc;
     CKK(mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream));
@@ -1071,7 +1105,7 @@ int mb_monodomain_sync(mb_monodomain *m) {
 int mb_solve_all_volumes_odes(mb_monodomain *m) {
     if (!m) return set_err(MB_ERR_ARG, "null");
     if (m->phase != 0) return set_err(MB_ERR_STATE, "ODE step already taken for this time step");
-    CKK(mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
+    CKK(step_ode(m));
     m->phase = 1;
     return MB_OK;
 }
@@ -1159,6 +1193,34 @@ int mb_monodomain_get_state(mb_monodomain *m, double *state_host) {
     CK(cudaStreamSynchronize(m->stream));
     cudaFree(d);
     return MB_OK;
+}
+
+int mb_monodomain_get_ecg(mb_monodomain *m, int64_t first, int64_t n, double *times, double *values,
+                          int64_t *records) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    if (!m->use_ecg) return set_err(MB_ERR_STATE, "the ECG is off (ecg_rate = 0)");
+    mb_ctrl c;
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaMemcpy(&c, m->d_ctrl, sizeof c, cudaMemcpyDeviceToHost));
+    if (records) *records = c.ecg_count;
+    if (n <= 0) return MB_OK;
+    if (first < 0 || first + n > c.ecg_count)
+        return set_err(MB_ERR_ARG, "ECG records %lld..%lld requested, %lld taken", (long long)first,
+                       (long long)(first + n - 1), (long long)c.ecg_count);
+    const int nl = m->ecg.n_leads;
+    const size_t row = (size_t)(1 + nl);
+    double *tmp = (double *)malloc((size_t)n * row * sizeof(double));
+    if (!tmp) return set_err(MB_ERR_NOMEM, "host memory");
+    cudaError_t e = cudaMemcpy(tmp, m->d_ecg_log + (size_t)first * row, (size_t)n * row * sizeof(double),
+                               cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        for (int64_t r = 0; r < n; ++r) {
+            if (times) times[r] = tmp[(size_t)r * row];
+            if (values)
+                for (int l = 0; l < nl; ++l) values[(size_t)r * nl + l] = tmp[(size_t)r * row + 1 + l];
+        }
+    free(tmp);
+    return e == cudaSuccess ? MB_OK : set_err(MB_ERR_CUDA, "ECG read-back: %s", cudaGetErrorString(e));
 }
 
 int mb_monodomain_get_activation(mb_monodomain *m, float *first, float *last, float *apd90, int32_t *count) {
@@ -1249,7 +1311,7 @@ int mb_monodomain_profile_steps(mb_monodomain *m, int n, double *ode_ms, double 
     long its = 0;
     for (int i = 0; i < n; ++i) {
         CK(cudaEventRecord(m->ev[0], m->stream));
-        CKK(mbk_ode_step(&m->ode, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
+        CKK(step_ode(m));
         CK(cudaEventRecord(m->ev[1], m->stream));
         {
             int rc = cg_enqueue(m);

@@ -80,7 +80,9 @@ def build_desc(nx: int, ny: int, nz: int, dx: float = 100.0, dy: float = 100.0, 
                initial_state: Optional[np.ndarray] = None, cg_tolerance: float = 1e-16,
                cg_max_iterations: int = 200, use_preconditioner: bool = True,
                stims: Sequence[Stim] = (), initial_v: float = float("nan"), track_activation: bool = False,
-               activation_threshold: float = -30.0, activation_min_interval: float = 10.0) -> Tuple[MbDesc, list]:
+               activation_threshold: float = -30.0, activation_min_interval: float = 10.0,
+               ecg_leads: Optional[Sequence[Sequence[float]]] = None, ecg_rate: int = 1, ecg_sigma_b: float = 1.0,
+               ecg_capacity: int = 100000) -> Tuple[MbDesc, list]:
     """The C-ABI tissue description (mb_monodomain_desc) for these arguments,
     with the arrays it points to (keep them alive while the description is
     in use).  Arrays given per cell are in grid order."""
@@ -135,6 +137,14 @@ def build_desc(nx: int, ny: int, nz: int, dx: float = 100.0, dy: float = 100.0, 
     d.track_activation = 1 if track_activation else 0
     d.activation_threshold = activation_threshold
     d.activation_min_interval = activation_min_interval
+    if ecg_leads is not None:
+        leads = np.ascontiguousarray(np.asarray(ecg_leads, dtype=np.float64).reshape(-1, 3))
+        keep.append(leads)
+        d.ecg_rate = int(ecg_rate)
+        d.ecg_n_leads = leads.shape[0]
+        d.ecg_leads = leads.ctypes.data
+        d.ecg_sigma_b = float(ecg_sigma_b)
+        d.ecg_capacity = int(ecg_capacity)
     return d, keep
 
 
@@ -155,7 +165,9 @@ class Tissue:
                  initial_state: Optional[np.ndarray] = None, cg_tolerance: float = 1e-16,
                  cg_max_iterations: int = 200, use_preconditioner: bool = True,
                  stims: Sequence[Stim] = (), initial_v: float = float("nan"), track_activation: bool = False,
-                 activation_threshold: float = -30.0, activation_min_interval: float = 10.0):
+                 activation_threshold: float = -30.0, activation_min_interval: float = 10.0,
+                 ecg_leads: Optional[Sequence[Sequence[float]]] = None, ecg_rate: int = 1, ecg_sigma_b: float = 1.0,
+                 ecg_capacity: int = 100000):
         self.shape = (nz, ny, nx)
         self.n = nx * ny * nz
         d, keep = build_desc(nx, ny, nz, dx, dy, dz, active=active, dt_pde=dt_pde, dt_ode=dt_ode, beta=beta,
@@ -166,9 +178,11 @@ class Tissue:
                              cg_tolerance=cg_tolerance, cg_max_iterations=cg_max_iterations,
                              use_preconditioner=use_preconditioner, stims=stims, initial_v=initial_v,
                              track_activation=track_activation, activation_threshold=activation_threshold,
-                             activation_min_interval=activation_min_interval)
+                             activation_min_interval=activation_min_interval, ecg_leads=ecg_leads,
+                             ecg_rate=ecg_rate, ecg_sigma_b=ecg_sigma_b, ecg_capacity=ecg_capacity)
         self.model = model
         self.precision = precision
+        self._n_leads = 0 if ecg_leads is None else int(np.asarray(ecg_leads).reshape(-1, 3).shape[0])
         self.active = None if active is None else np.asarray(active, dtype=bool).reshape(-1).copy()
         h = C.c_void_p()
         check(lib.mb_monodomain_create(C.byref(h), C.byref(d)))
@@ -242,6 +256,19 @@ class Tissue:
     def save_v(self, path: str, binary: bool = False):
         """V of the active cells in the reference's save_as_text_or_binary format."""
         check(lib.mb_monodomain_save_v(self._h, path.encode(), 1 if binary else 0))
+
+    def ecg(self):
+        """Pseudo-bidomain ECG records taken so far (needs ecg_leads): the
+        loop time of each record (ms) and the leads' values, one row per
+        record (the columns of the reference's ecg.txt)."""
+        n = C.c_int64()
+        check(lib.mb_monodomain_get_ecg(self._h, 0, 0, None, None, C.byref(n)))
+        t = np.empty(n.value, dtype=np.float64)
+        nl = self._n_leads
+        vals = np.empty((n.value, nl), dtype=np.float64)
+        if n.value:
+            check(lib.mb_monodomain_get_ecg(self._h, 0, n.value, _ptr(t), _ptr(vals), C.byref(n)))
+        return t, vals
 
     def activation(self) -> dict:
         """Activation times tracked on the device (needs track_activation):

@@ -163,3 +163,43 @@ def torord_initial_state(celltype: int = 0) -> np.ndarray:
 
 def loop_steps(final_time: float, dt: float) -> int:
     return load().orc_loop_steps(final_time, dt)
+
+
+def pseudo_bidomain_ecg(v: np.ndarray, nx: int, ny: int, nz: int, leads, sigma_b: float,
+                        dx: float = 100.0, dy: float = 100.0, dz: float = 100.0,
+                        active: Optional[np.ndarray] = None) -> np.ndarray:
+    """Pseudo-bidomain ECG of the grid-order V at the given electrodes, as
+    ecg_library/ecg.c computes it on a cuboid mesh:
+      - assembly_divergent / fill_element (ecg.c:36-43, 149-172): per active
+        cell, each face neighbour that is an active cell inside the domain
+        gets value_ecg = -m and the diagonal +m, with m = dx dy / dz for
+        every face direction;
+      - pseudo_bidomain_cpu (ecg.c:264-307): beta_im = sum(value_ecg v) / vol,
+        lead = -(1 / (4 pi sigma_b)) sum_cells beta_im / |x_cell - lead| vol,
+        cell centres at ((i + 1/2) dx, (j + 1/2) dy, (k + 1/2) dz).
+    Test infrastructure: the checker of the device ECG."""
+    n = nx * ny * nz
+    act = np.ones(n, bool) if active is None else np.asarray(active).astype(bool)
+    V = np.asarray(v, float).reshape(nz, ny, nx)
+    A = act.reshape(nz, ny, nx)
+    m = (dx * dy) / dz
+    lap = np.zeros_like(V)
+    for axis in range(3):
+        for shift in (1, -1):
+            nb = np.roll(V, shift, axis=axis)
+            na = np.roll(A, shift, axis=axis)
+            edge = [slice(None)] * 3
+            edge[axis] = 0 if shift == 1 else -1
+            ok = A & na
+            ok[tuple(edge)] = False
+            lap += np.where(ok, m * (V - np.where(ok, nb, 0.0)), 0.0)
+    vol = dx * dy * dz
+    beta = np.where(A, lap / vol, 0.0)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    cx, cy, cz = (i + 0.5) * dx, (j + 0.5) * dy, (k + 0.5) * dz
+    scale = 1.0 / (4.0 * np.pi * sigma_b)
+    out = []
+    for (ex, ey, ez) in leads:
+        dist = np.sqrt((ex - cx) ** 2 + (ey - cy) ** 2 + (ez - cz) ** 2)
+        out.append(-scale * np.sum(np.where(A, beta / dist * vol, 0.0)))
+    return np.array(out)

@@ -8,7 +8,7 @@ Each case writes an ini file, runs oracle/_ref/bin/MonoAlg3D with the binary
 V writer (save_as_text_or_binary, binary=true: centre, half sizes and V as
 doubles per active cell), maps the cells to grid order by their centres and
 stores V every `print_rate` steps plus the CG iterations and error of every
-step from the solver log.  Runs only where the reference tree is mounted; the
+step from the solver log (and, for the ECG case, the reference's ecg.txt).  Runs only where the reference tree is mounted; the
 fixtures are committed and the tests read only them.
 """
 from __future__ import annotations
@@ -41,6 +41,10 @@ CASES = {
     "tt2006_aniso_x": dict(nx=32, ny=8, nz=2, model="tt2006", assembly="anisotropic", fibre_deg=0.0, sim_ms=12.0),
     # anisotropic assembly, fibres at 30 degrees in the xy plane (cross terms)
     "tt2006_aniso_30": dict(nx=32, ny=8, nz=3, model="tt2006", assembly="anisotropic", fibre_deg=30.0, sim_ms=12.0),
+    # pseudo-bidomain ECG (ecg_library/ecg.c) every 5 steps at three electrodes around the slab
+    "tt2006_ecg": dict(nx=32, ny=16, nz=3, model="tt2006", assembly="homogeneous", sim_ms=30.0,
+                       ecg=dict(leads=[[-500.0, 800.0, 150.0], [3700.0, 800.0, 150.0], [1600.0, -400.0, 150.0]],
+                                sigma_b=1.0, calc_rate=5)),
 }
 
 DX = 100.0
@@ -60,9 +64,15 @@ def ini_text(case: dict, out_dir: str) -> str:
                     "sigma_l=0.0002\nsigma_t=0.00005\nsigma_n=0.00005\n"
                     f"f=[{float(np.cos(th))!r},{float(np.sin(th))!r},0.0]\n")
     extra = ""
+    if case.get("ecg"):
+        e = case["ecg"]
+        leads = "".join(f"lead{i + 1}={x!r},{y!r},{z!r}\n" for i, (x, y, z) in enumerate(e["leads"]))
+        extra += ("[calc_ecg]\nmain_function=pseudo_bidomain\ninit_function=init_pseudo_bidomain\n"
+                  f"end_function=end_pseudo_bidomain\ncalc_rate={e['calc_rate']}\n{leads}sigma_b={e['sigma_b']!r}\n"
+                  f"use_gpu=no\nlibrary_file={LIBS}/libdefault_calc_ecg.so\n\n")
     if case.get("extra_data"):
-        extra = ("[extra_data]\nmain_function=set_extra_data_mixed_torord_fkatp_epi_mid_endo\n"
-                 f"library_file={LIBS}/libdefault_extra_data.so\n")
+        extra += ("[extra_data]\nmain_function=set_extra_data_mixed_torord_fkatp_epi_mid_endo\n"
+                  f"library_file={LIBS}/libdefault_extra_data.so\n")
     return f"""[main]
 num_threads=4
 dt_pde={DT}
@@ -150,8 +160,14 @@ def run_case(name: str, case: dict) -> dict:
         counts = [c for c in counts if c % PRINT_RATE == 0]
         V = np.stack([read_bin(os.path.join(out_dir, f"V_it_{c}.bin"), case["nx"], case["ny"], case["nz"])
                       for c in counts])
-    return dict(V=V, counts=np.array(counts), its=np.array(its), errors=np.array(errs),
-                config=json.dumps(dict(case, dx=DX, dt=DT, print_rate=PRINT_RATE)))
+        res = dict(V=V, counts=np.array(counts), its=np.array(its), errors=np.array(errs),
+                   config=json.dumps(dict(case, dx=DX, dt=DT, print_rate=PRINT_RATE)))
+        if case.get("ecg"):
+            # ecg.txt: time and one value per lead per line, "%lf" (ecg.c:286-306)
+            rows = np.loadtxt(os.path.join(out_dir, "ecg.txt"), ndmin=2)
+            res["ecg_t"] = rows[:, 0]
+            res["ecg"] = rows[:, 1:]
+    return res
 
 
 def main(names=None):

@@ -95,3 +95,24 @@ def test_pcg_against_dense_solve():
     x, its, err = oracle.pcg(rp, col, val, b, np.zeros_like(b), tol=1e-24, max_its=500)
     np.testing.assert_allclose(x, np.linalg.solve(A, b), rtol=1e-10, atol=1e-12)
     assert err <= 1e-24 and 1 < its < 500
+
+
+def test_ecg_restatement_matches_reference():
+    """The oracle's pseudo-bidomain ECG, evaluated on the reference's own V
+    dumps, against the ecg.txt the reference wrote at the same steps (its
+    "%lf" output: six decimals)."""
+    import json
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tt2006_ecg.npz"))
+    cfg = json.loads(str(g["config"]))
+    e = cfg["ecg"]
+    rate = e["calc_rate"]
+    checked = 0
+    for c, v in zip(g["counts"], g["V"]):
+        if c % rate:
+            continue
+        got = oracle.pseudo_bidomain_ecg(v, cfg["nx"], cfg["ny"], cfg["nz"], e["leads"], e["sigma_b"])
+        ref = g["ecg"][c // rate]
+        assert np.allclose(got, ref, rtol=0, atol=6e-7), f"count {c}: {got} vs {ref}"
+        checked += 1
+    assert checked >= 20
+    assert np.abs(g["ecg"]).max() > 0.5        # the wave's signal, not only zeros
