@@ -338,6 +338,20 @@ int mb_monodomain_time_steps(mb_monodomain *m, int n, double *ms);
 int mb_monodomain_time_steps_host(mb_monodomain *m, int n, const double *stim_host, double *v_host,
                                   double *ms);
 
+/* Pipelined reference-host steps (no reference counterpart; the same work
+ * and copies as mb_monodomain_step_host): call k copies its stimulus in and
+ * its V out on a copy stream that runs under the compute of the neighbouring
+ * steps, and returns once the copies of call k - 1 are done (its V is in its
+ * host buffer, its buffers may be refilled), so the caller alternates two
+ * pairs of host buffers (pinned, for the copies to overlap).
+ * mb_monodomain_host_wait completes the last call's copies.  The timed form
+ * runs n steps with buffer pairs (stim0, v0) and (stim1, v1) and reports the
+ * device time from the first copy to the last.                             */
+int mb_monodomain_step_host_async(mb_monodomain *m, const double *stim_host, double *v_host);
+int mb_monodomain_host_wait(mb_monodomain *m);
+int mb_monodomain_time_steps_host_async(mb_monodomain *m, int n, const double *stim0, const double *stim1,
+                                        double *v0, double *v1, double *ms);
+
 /* Launch choices made at creation by timing: the ODE kernel's variant
  * (0..5 = one-cell-per-thread launches with at least 1..6 resident 128-thread
  * blocks per SM, 6..9 = staged persistent launches with at least 1..4), the

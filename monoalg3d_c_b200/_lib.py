@@ -45,7 +45,8 @@ EXPORTED = [
     "mb_monodomain_step", "mb_monodomain_sync", "mb_solve_all_volumes_odes",
     "mb_update_monodomain_default", "mb_conjugate_gradient", "mb_advance_time",
     "mb_monodomain_step_host", "mb_monodomain_get_v", "mb_monodomain_set_v", "mb_monodomain_get_activation",
-    "mb_monodomain_get_ecg",
+    "mb_monodomain_get_ecg", "mb_monodomain_step_host_async", "mb_monodomain_host_wait",
+    "mb_monodomain_time_steps_host_async",
     "mb_batch_pack", "mb_monodomain_checkpoint_bytes", "mb_monodomain_checkpoint", "mb_monodomain_restore",
     "mb_monodomain_save_v", "mb_adjoint_create", "mb_adjoint_forward", "mb_adjoint_backward", "mb_adjoint_destroy",
     "mb_monodomain_get_state", "mb_monodomain_info", "mb_monodomain_step_stats",
@@ -148,6 +149,9 @@ def _load() -> C.CDLL:
         "mb_monodomain_get_v": (i32, [vp, vp]),
         "mb_monodomain_get_activation": (i32, [vp, vp, vp, vp, vp]),
         "mb_monodomain_get_ecg": (i32, [vp, i64, i64, vp, vp, P(i64)]),
+        "mb_monodomain_step_host_async": (i32, [vp, vp, vp]),
+        "mb_monodomain_host_wait": (i32, [vp]),
+        "mb_monodomain_time_steps_host_async": (i32, [vp, i32, vp, vp, vp, vp, P(dbl)]),
         "mb_batch_pack": (i32, [i32, vp, vp, P(i32), P(i32), vp, vp]),
         "mb_monodomain_checkpoint_bytes": (i32, [vp, P(C.c_size_t)]),
         "mb_monodomain_checkpoint": (i32, [vp, vp, C.c_size_t]),

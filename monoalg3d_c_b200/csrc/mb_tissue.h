@@ -68,6 +68,15 @@ struct mb_monodomain {
     int use_graphs;
     int phase;            /* split-API state: 0 idle, 1 ODE done, 2 RHS formed */
     cudaEvent_t ev[4];
+    /* pipelined host-buffer steps (mb_monodomain_step_host_async): one copy
+     * stream per direction, two slots of device stimulus and V snapshot, and
+     * per slot the events stimulus-copied, ODE-done (slot stimulus free),
+     * V-snapshot-ready and V-copied (slot snapshot and host buffer free) */
+    cudaStream_t copy_stream;     /* device -> host (V) */
+    cudaStream_t h2d_stream;      /* host -> device (stimulus) */
+    double *d_stim2[2], *d_vsnap[2];
+    cudaEvent_t hev[4][2];
+    int64_t host_calls;
 };
 
 /* Device-to-device snapshot of the loop state (V, V*, the ODE state rows and

@@ -304,9 +304,14 @@ void mb_monodomain_destroy(mb_monodomain *m) {
                     m->d_mask, m->d_cells, m->d_v, m->d_vstar, m->d_r, m->d_p, m->d_r32, m->d_p32,
                     m->d_partials, m->d_sv64, m->d_sv32, m->d_stim_bits, m->d_celltype, m->d_scale,
                     m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_code, m->d_rowid, m->d_act,
-                    m->d_stim_host, m->d_ctrl, m->d_log};
+                    m->d_stim_host, m->d_ctrl, m->d_log, m->d_stim2[0], m->d_stim2[1], m->d_vsnap[0],
+                    m->d_vsnap[1]};
     for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
     for (int i = 0; i < 4; ++i) if (m->ev[i]) cudaEventDestroy(m->ev[i]);
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 2; ++j) if (m->hev[i][j]) cudaEventDestroy(m->hev[i][j]);
+    if (m->copy_stream) cudaStreamDestroy(m->copy_stream);
+    if (m->h2d_stream) cudaStreamDestroy(m->h2d_stream);
     if (m->stream) cudaStreamDestroy(m->stream);
     free(m->h_mask);
     free(m);
@@ -1151,6 +1156,7 @@ int mb_monodomain_step_host(mb_monodomain *m, const double *stim_host, double *v
                            m->stream));
         o.stim_host = m->d_stim_host;
     }
+    if (m->use_ecg) CKK(mbk_ecg(&m->st, m->d_v, &m->ecg, m->d_ctrl, m->stream));
     CKK(mbk_ode_step(&o, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
     {
         int rc = cg_enqueue(m);
@@ -1161,6 +1167,106 @@ int mb_monodomain_step_host(mb_monodomain *m, const double *stim_host, double *v
         CK(cudaMemcpyAsync(v_host, m->d_v, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
         CK(cudaStreamSynchronize(m->stream));
     }
+    return MB_OK;
+}
+
+/* Pipelined form of mb_monodomain_step_host.  Call k uses slot k % 2: the
+ * stimulus is copied into the slot's device buffer on the host-to-device
+ * stream (after the ODE of call k - 2 has read that buffer) while step k - 1
+ * still runs, the step runs on the tissue's stream, V is snapshotted into
+ * the slot's device buffer and copied to v_host on the device-to-host stream
+ * while the next step runs; the two directions do not queue behind each
+ * other.  The call returns once
+ * the copies of call k - 1 are complete (its V is in its host buffer and its
+ * buffers may be refilled), so the caller alternates two pairs of host
+ * buffers (pinned memory for the copies to overlap); the last call's copies
+ * are complete after mb_monodomain_host_wait. */
+static int host_pipeline_init(mb_monodomain *m) {
+    if (m->copy_stream) return MB_OK;
+    const size_t sb = (size_t)m->n_active * sizeof(double), vb = (size_t)m->n * sizeof(double);
+    cudaError_t e = cudaStreamCreateWithFlags(&m->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&m->h2d_stream, cudaStreamNonBlocking);
+    for (int j = 0; j < 2 && e == cudaSuccess; ++j) {
+        e = cudaMalloc((void **)&m->d_stim2[j], sb ? sb : 8);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&m->d_vsnap[j], vb);
+        for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&m->hev[i][j], cudaEventDisableTiming);
+        /* every slot starts free: record its events once */
+        for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventRecord(m->hev[i][j], m->copy_stream);
+    }
+    if (e != cudaSuccess) return set_err(MB_ERR_CUDA, "host pipeline: %s", cudaGetErrorString(e));
+    return MB_OK;
+}
+
+enum { HEV_STIM = 0, HEV_ODE = 1, HEV_VREADY = 2, HEV_VDONE = 3 };
+
+int mb_monodomain_step_host_async(mb_monodomain *m, const double *stim_host, double *v_host) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    int rc = host_pipeline_init(m);
+    if (rc) return rc;
+    const int s = (int)(m->host_calls & 1);
+    /* slot s was last used by call k - 2, whose copies call k - 1 waited for */
+    mb_ode_dev o = m->ode;
+    if (stim_host) {
+        CK(cudaStreamWaitEvent(m->h2d_stream, m->hev[HEV_ODE][s], 0));
+        CK(cudaMemcpyAsync(m->d_stim2[s], stim_host, (size_t)m->n_active * sizeof(double), cudaMemcpyHostToDevice,
+                           m->h2d_stream));
+        CK(cudaEventRecord(m->hev[HEV_STIM][s], m->h2d_stream));
+        CK(cudaStreamWaitEvent(m->stream, m->hev[HEV_STIM][s], 0));
+        o.stim_host = m->d_stim2[s];
+    }
+    if (m->use_ecg) CKK(mbk_ecg(&m->st, m->d_v, &m->ecg, m->d_ctrl, m->stream));
+    CKK(mbk_ode_step(&o, m->d_ctrl, m->d_v, m->d_vstar, m->stream));
+    CK(cudaEventRecord(m->hev[HEV_ODE][s], m->stream));
+    rc = cg_enqueue(m);
+    if (rc) return rc;
+    CKK(mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream));
+    if (v_host) {
+        CK(cudaMemcpyAsync(m->d_vsnap[s], m->d_v, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream));
+        CK(cudaEventRecord(m->hev[HEV_VREADY][s], m->stream));
+        CK(cudaStreamWaitEvent(m->copy_stream, m->hev[HEV_VREADY][s], 0));
+        CK(cudaMemcpyAsync(v_host, m->d_vsnap[s], (size_t)m->n * sizeof(double), cudaMemcpyDeviceToHost,
+                           m->copy_stream));
+    }
+    CK(cudaEventRecord(m->hev[HEV_VDONE][s], m->copy_stream));
+    m->host_calls += 1;
+    /* the copies of call k - 1 (they ran under this step's compute) */
+    CK(cudaEventSynchronize(m->hev[HEV_VDONE][1 - s]));
+    return MB_OK;
+}
+
+int mb_monodomain_host_wait(mb_monodomain *m) {
+    if (!m) return set_err(MB_ERR_ARG, "null");
+    if (m->copy_stream) CK(cudaStreamSynchronize(m->copy_stream));
+    if (m->h2d_stream) CK(cudaStreamSynchronize(m->h2d_stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return MB_OK;
+}
+
+/* n pipelined host-buffer steps alternating the two buffer pairs, timed from
+ * before the first copy to after the last copy (CUDA events on both streams). */
+int mb_monodomain_time_steps_host_async(mb_monodomain *m, int n, const double *stim0, const double *stim1,
+                                        double *v0, double *v1, double *ms) {
+    if (!m || n <= 0 || !ms) return set_err(MB_ERR_ARG, "bad arguments");
+    int rc = host_pipeline_init(m);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(m->copy_stream));
+    CK(cudaStreamSynchronize(m->h2d_stream));
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaEventRecord(m->ev[2], m->stream));
+    CK(cudaStreamWaitEvent(m->copy_stream, m->ev[2], 0));
+    CK(cudaStreamWaitEvent(m->h2d_stream, m->ev[2], 0));
+    for (int i = 0; i < n; ++i) {
+        const int s = (int)(m->host_calls & 1);
+        rc = mb_monodomain_step_host_async(m, s ? stim1 : stim0, s ? v1 : v0);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(m->hev[HEV_VDONE][0], m->copy_stream));
+    CK(cudaStreamWaitEvent(m->stream, m->hev[HEV_VDONE][0], 0));
+    CK(cudaEventRecord(m->ev[3], m->stream));
+    CK(cudaEventSynchronize(m->ev[3]));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, m->ev[2], m->ev[3]));
+    *ms = t;
     return MB_OK;
 }
 

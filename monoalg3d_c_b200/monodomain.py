@@ -314,6 +314,14 @@ class Tissue:
         check(lib.mb_monodomain_time_steps_host(self._h, int(n), stim_ptr, v_ptr, C.byref(ms)))
         return ms.value
 
+    def time_steps_host_async(self, n: int, stim0: int, stim1: int, v0: int, v1: int) -> float:
+        """Device milliseconds of n pipelined host-buffer steps alternating the
+        buffer pairs (stim0, v0) and (stim1, v1) (raw addresses of pinned memory)."""
+        ms = C.c_double()
+        check(lib.mb_monodomain_time_steps_host_async(self._h, int(n), C.c_void_p(stim0), C.c_void_p(stim1),
+                                                      C.c_void_p(v0), C.c_void_p(v1), C.byref(ms)))
+        return ms.value
+
     def tuning(self):
         v, b, pc = C.c_int(), C.c_int(), C.c_int()
         check(lib.mb_monodomain_tuning(self._h, C.byref(v), C.byref(b), C.byref(pc)))
