@@ -355,9 +355,11 @@ int mb_monodomain_time_steps_host_async(mb_monodomain *m, int n, const double *s
 /* Launch choices made at creation by timing: the ODE kernel's variant
  * (0..5 = one-cell-per-thread launches with at least 1..6 resident 128-thread
  * blocks per SM, 6..9 = staged persistent launches with at least 1..4), the
- * CG grid size and the CG kernel (-1 = graph of separate kernels, 0.. =
- * launch shape of the flat persistent kernel, 100 = the 2.5D tiled
- * persistent kernel, 200 = the resident tile-column kernel). */
+ * CG grid size and the CG kernel (-1 = graph of separate kernels, 0..19 =
+ * launch shape of the flat persistent kernel -- 0..9 with a contiguous range
+ * of cells per block, 10..19 the same shapes sweeping the grid interleaved --,
+ * 100 = the 2.5D tiled persistent kernel, 200 = the resident tile-column
+ * kernel). */
 int mb_monodomain_tuning(mb_monodomain *m, int *ode_variant, int *cg_blocks, int *cg_kernel);
 
 /* ---- general sparse CG (test_solvers.c fixtures) ---------------------- */

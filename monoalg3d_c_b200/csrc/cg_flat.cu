@@ -94,7 +94,8 @@ __device__ __forceinline__ T row_apply(const mb_stencil_dev &st, const Row7<T, K
 
 // 27-point rows (kind 2) from the per-plane class table; the product is
 // formed while gathering.  Missing neighbours have zero coefficients in the
-// table and are not loaded.
+// table and are not loaded; entries that are zero in every row of the table
+// (st.nzmask) are not read at all.
 template <typename T>
 struct Row27 {
     T pc, ap;
@@ -116,6 +117,7 @@ __device__ __forceinline__ Row27<T> gather27(const mb_stencil_dev &st, uint32_t 
 #pragma unroll
             for (int dx = -1; dx <= 1; ++dx) {
                 const int q = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+                if (!((st.nzmask >> q) & 1u)) continue;     // zero in every row
                 const T c = sizeof(T) == 8 ? T(__ldg(st.table + row + q)) : T(__ldg(st.table32 + row + q));
                 if (q == 13) acc += c * R.pc;
                 else if (c != T(0)) acc += c * pf((uint32_t)((int)g + dx + sy * dy + sz * dz));
@@ -145,26 +147,52 @@ __device__ __forceinline__ void block_chunk(uint32_t n, uint32_t &c0, uint32_t &
     c1 = min(n, c0 + chunk);
 }
 
+// The units (cells or groups) a thread visits in a pass, in rounds of
+// per_round = U x blockDim units per block: unit base + u blockDim (u < U) for
+// base = start, start + step, ... below end.
+//   ORD 0: each block sweeps its own contiguous range (block_chunk).
+//   ORD 1: interleaved -- round r of block b covers units
+//          [(r G + b) per_round, (r G + b + 1) per_round), G blocks, so the
+//          whole grid moves through the cells together and the rows a round
+//          reads one z-plane away were read a few rounds before (still in
+//          L2 when a pass streams far more than L2 holds).
+template <int ORD>
+struct Sweep {
+    uint32_t start, end, step;
+    __device__ __forceinline__ Sweep(uint32_t units, uint32_t per_round) {
+        if constexpr (ORD == 0) {
+            uint32_t c0, c1;
+            block_chunk(units, c0, c1);
+            start = c0 + threadIdx.x;
+            end = c1;
+            step = per_round;
+        } else {
+            start = blockIdx.x * per_round + threadIdx.x;
+            end = units;
+            step = gridDim.x * per_round;
+        }
+    }
+};
+
 // A pass over the active cells: each thread takes U cells of the block's range
 // at a time and gathers all U rows (their loads in flight together) before
 // using them.
-template <typename T, int KIND, int NT, int U, typename PF, typename ACT>
+template <typename T, int KIND, int NT, int U, int ORD, typename PF, typename ACT>
 __device__ __forceinline__ void pass(const mb_stencil_dev &st, PF pf, ACT act) {
     const uint32_t n = (uint32_t)st.nx * st.ny * st.nz;
-    uint32_t c0, c1;
-    block_chunk(n, c0, c1);
     const uint32_t nt = blockDim.x;     // <= NT: the host sizes blocks to whole rounds
-    for (uint32_t base = c0 + threadIdx.x; base < c1; base += U * nt) {
+    const Sweep<ORD> sw(n, U * nt);
+    for (uint32_t base = sw.start; base < sw.end; base += sw.step) {
         decltype(gather<T, KIND>(st, 0u, pf)) rows[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t g = base + u * nt;
-            rows[u] = gather<T, KIND>(st, g < c1 ? g : base, pf);
+            rows[u] = gather<T, KIND>(st, g < sw.end ? g : base, pf);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t g = base + u * nt;
-            if (g < c1 && (rows[u].m & ACTIVE)) act(g, rows[u]);
+            if (g < sw.end && (rows[u].m & ACTIVE)) act(g, rows[u]);
         }
     }
 }
@@ -219,7 +247,8 @@ __device__ __forceinline__ void fill_inv_table(const mb_stencil_dev &st, typenam
 // on each side for the x neighbours of the group's end cells.  Row indices
 // are clamped into the grid; values of neighbours that do not couple are
 // discarded (kinds 0, 1) or multiplied by the zero coefficients the class
-// table holds for them (kind 2).  Sums run in the same order as the
+// table holds for them (kind 2; rows and entries that are zero in every row
+// of the table are skipped).  Sums run in the same order as the
 // one-cell-per-thread rows above, so both forms give the same values.
 
 template <typename T>
@@ -282,6 +311,10 @@ __device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, co
         for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
             for (int dy = -1; dy <= 1; ++dy) {
+                // entries dx = -1, 0, +1 of this row that are non-zero
+                // somewhere in the table (the same for every thread)
+                const unsigned rb = (st.nzmask >> ((dz + 1) * 9 + (dy + 1) * 3)) & 7u;
+                if (!rb) continue;
                 uint32_t b = g0;
                 if (dz < 0) b = b >= sz ? b - sz : g0;
                 if (dz > 0) b = b + sz < n ? b + sz : g0;
@@ -289,12 +322,13 @@ __device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, co
                 if (dy > 0) b = b + sy < n ? b + sy : g0;
                 const Vec4<T> mid = (dz == 0 && dy == 0) ? pc : f.row(b);
                 T w[6];
-                w[0] = f.at(b > 0 ? b - 1 : b);
+                w[0] = (rb & 1u) ? f.at(b > 0 ? b - 1 : b) : T(0);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) w[k + 1] = mid.v[k];
-                w[5] = f.at(b + 4 < n ? b + 4 : b);
+                w[5] = (rb & 4u) ? f.at(b + 4 < n ? b + 4 : b) : T(0);
 #pragma unroll
                 for (int dx = -1; dx <= 1; ++dx) {
+                    if (!((rb >> (dx + 1)) & 1u)) continue;
                     const int q = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
                     const T c0 = sizeof(T) == 8 ? T(__ldg(st.table + rw[0] + q)) : T(__ldg(st.table32 + rw[0] + q));
 #pragma unroll
@@ -354,23 +388,22 @@ __device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, co
 // A pass over the groups of the block's range: each thread takes U groups at
 // a time and forms all U products (their loads in flight together) before
 // act(g0, pc, ap, m) runs for each.
-template <typename T, int KIND, int NT, int U, typename F, typename ACT>
+template <typename T, int KIND, int NT, int U, int ORD, typename F, typename ACT>
 __device__ __forceinline__ void pass4(const mb_stencil_dev &st, const F &f, ACT act) {
     const uint32_t groups = ((uint32_t)st.nx * st.ny * st.nz) >> 2;
-    uint32_t c0, c1;
-    block_chunk(groups, c0, c1);
     const uint32_t nt = blockDim.x;     // <= NT: the host sizes blocks to whole rounds
-    for (uint32_t q = c0 + threadIdx.x; q < c1; q += U * nt) {
+    const Sweep<ORD> sw(groups, U * nt);
+    for (uint32_t q = sw.start; q < sw.end; q += sw.step) {
         Vec4<T> pc[U], ap[U];
         unsigned m[U][4];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t qq = q + u * nt;
-            apply4<T, KIND>(st, (qq < c1 ? qq : q) << 2, f, pc[u], ap[u], m[u]);
+            apply4<T, KIND>(st, (qq < sw.end ? qq : q) << 2, f, pc[u], ap[u], m[u]);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            if (q + u * nt < c1) act((q + u * nt) << 2, pc[u], ap[u], m[u]);
+            if (q + u * nt < sw.end) act((q + u * nt) << 2, pc[u], ap[u], m[u]);
     }
 }
 
@@ -378,7 +411,7 @@ __device__ __forceinline__ void pass4(const mb_stencil_dev &st, const F &f, ACT 
 
 // FP64 true residual r = b - A x; stores r (in T), z and p = z; accumulates
 // r.z (T products, FP64 sums), r.r of the stored r, and the FP64 r.r.
-template <bool MIXED, int KIND, int NT, int U, bool VEC>
+template <bool MIXED, int KIND, int NT, int U, bool VEC, int ORD>
 __device__ __forceinline__ void residual_pass(const Args &a, typename Prec<MIXED>::T *r,
                                               typename Prec<MIXED>::T *p, bool pre,
                                               const typename Prec<MIXED>::T *itab, double (&acc)[3]) {
@@ -386,7 +419,7 @@ __device__ __forceinline__ void residual_pass(const Args &a, typename Prec<MIXED
     const mb_stencil_dev &st = a.st;
     const double *__restrict__ x = a.x;
     if constexpr (VEC) {
-        pass4<double, KIND, NT, U>(st, Plain<double>{x}, [&](uint32_t g0, const Vec4<double> &xc, const Vec4<double> &ax,
+        pass4<double, KIND, NT, U, ORD>(st, Plain<double>{x}, [&](uint32_t g0, const Vec4<double> &xc, const Vec4<double> &ax,
                                                         const unsigned (&m)[4]) {
             Vec4<T> rv = ld4(r, g0), pv = ld4(p, g0);
 #pragma unroll
@@ -407,7 +440,7 @@ __device__ __forceinline__ void residual_pass(const Args &a, typename Prec<MIXED
             st4(p, g0, pv);
         });
     } else {
-        pass<double, KIND, NT, U>(st, [&](uint32_t q) { return x[q]; },
+        pass<double, KIND, NT, U, ORD>(st, [&](uint32_t q) { return x[q]; },
                                   [&](uint32_t g, const auto &row) {
                                       const double ax = product<double, KIND>(st, row);
                                       const double bb = a.b ? a.b[g] : st.alpha * a.vstar[g];
@@ -425,7 +458,7 @@ __device__ __forceinline__ void residual_pass(const Args &a, typename Prec<MIXED
 
 // Q: the direction (p_new = z + beta p_old, or p itself on a restart), stored
 // when new, A p stored for the U pass, and the partial sum of p.Ap.
-template <bool MIXED, int KIND, int NT, int U, bool VEC>
+template <bool MIXED, int KIND, int NT, int U, bool VEC, int ORD>
 __device__ __forceinline__ void q_pass(const Args &a, bool first, const typename Prec<MIXED>::T *po,
                                        typename Prec<MIXED>::T *pw, const typename Prec<MIXED>::T *zb,
                                        typename Prec<MIXED>::T *apb, double beta, double &q1) {
@@ -439,13 +472,13 @@ __device__ __forceinline__ void q_pass(const Args &a, bool first, const typename
                 if (m[k] & ACTIVE) q1 += (double)pc.v[k] * (double)ap.v[k];
         };
         if (first) {
-            pass4<T, KIND, NT, U>(st, Plain<T>{po}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
+            pass4<T, KIND, NT, U, ORD>(st, Plain<T>{po}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
                                                      const unsigned (&m)[4]) {
                 st4(apb, g0, ap);
                 dot(pc, ap, m);
             });
         } else {
-            pass4<T, KIND, NT, U>(st, Direction<T>{zb, po, bt}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
+            pass4<T, KIND, NT, U, ORD>(st, Direction<T>{zb, po, bt}, [&](uint32_t g0, const Vec4<T> &pc, const Vec4<T> &ap,
                                                                  const unsigned (&m)[4]) {
                 st4(pw, g0, pc);
                 st4(apb, g0, ap);
@@ -454,14 +487,14 @@ __device__ __forceinline__ void q_pass(const Args &a, bool first, const typename
         }
     } else {
         if (first) {
-            pass<T, KIND, NT, U>(st, [&](uint32_t q) { return po[q]; },
+            pass<T, KIND, NT, U, ORD>(st, [&](uint32_t q) { return po[q]; },
                                  [&](uint32_t g, const auto &row) {
                                      const T ap = product<T, KIND>(st, row);
                                      apb[g] = ap;
                                      q1 += (double)row.pc * (double)ap;
                                  });
         } else {
-            pass<T, KIND, NT, U>(st, [&](uint32_t q) { return zb[q] + bt * po[q]; },
+            pass<T, KIND, NT, U, ORD>(st, [&](uint32_t q) { return zb[q] + bt * po[q]; },
                                  [&](uint32_t g, const auto &row) {
                                      pw[g] = row.pc;
                                      const T ap = product<T, KIND>(st, row);
@@ -476,7 +509,7 @@ __device__ __forceinline__ void q_pass(const Args &a, bool first, const typename
 // partial sums of r.z and r.r.  A streaming pass: every value it reads is the
 // cell's own.  z of removed cells is stored as 0 (no active cell couples to
 // them).
-template <bool MIXED, int KIND, int NT, int U, bool VEC>
+template <bool MIXED, int KIND, int NT, int U, bool VEC, int ORD>
 __device__ __forceinline__ void u_pass(const Args &a, const typename Prec<MIXED>::T *pc_,
                                        const typename Prec<MIXED>::T *apb, typename Prec<MIXED>::T *r,
                                        typename Prec<MIXED>::T *zb, bool pre, const typename Prec<MIXED>::T *itab,
@@ -488,16 +521,15 @@ __device__ __forceinline__ void u_pass(const Args &a, const typename Prec<MIXED>
     const uint32_t n = (uint32_t)st.nx * st.ny * st.nz;
     const uint32_t nt = blockDim.x;
     if constexpr (VEC) {
-        uint32_t c0, c1;
-        block_chunk(n >> 2, c0, c1);
-        for (uint32_t q = c0 + threadIdx.x; q < c1; q += U * nt) {
+        const Sweep<ORD> sw(n >> 2, U * nt);
+        for (uint32_t q = sw.start; q < sw.end; q += sw.step) {
             Vec4<T> pv[U], av[U], rv[U], id[U];
             Vec4<double> xv[U];
             unsigned m[U][4];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const uint32_t qq = q + u * nt;
-                const uint32_t g0 = (qq < c1 ? qq : q) << 2;
+                const uint32_t g0 = (qq < sw.end ? qq : q) << 2;
                 if constexpr (KIND == 2) {
                     m[u][0] = m[u][1] = m[u][2] = m[u][3] = ACTIVE;
                 } else {
@@ -517,7 +549,7 @@ __device__ __forceinline__ void u_pass(const Args &a, const typename Prec<MIXED>
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                if (q + u * nt >= c1) continue;
+                if (q + u * nt >= sw.end) continue;
                 const uint32_t g0 = (q + u * nt) << 2;
                 Vec4<T> zv;
 #pragma unroll
@@ -543,16 +575,15 @@ __device__ __forceinline__ void u_pass(const Args &a, const typename Prec<MIXED>
             }
         }
     } else {
-        uint32_t c0, c1;
-        block_chunk(n, c0, c1);
-        for (uint32_t base = c0 + threadIdx.x; base < c1; base += U * nt) {
+        const Sweep<ORD> sw(n, U * nt);
+        for (uint32_t base = sw.start; base < sw.end; base += sw.step) {
             T pv[U], av[U], rv[U];
             double xv[U];
             unsigned m[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const uint32_t gg = base + u * nt;
-                const uint32_t g = gg < c1 ? gg : base;
+                const uint32_t g = gg < sw.end ? gg : base;
                 if constexpr (KIND == 2) m[u] = ACTIVE;
                 else m[u] = st.code[g];
                 pv[u] = pc_[g];
@@ -563,7 +594,7 @@ __device__ __forceinline__ void u_pass(const Args &a, const typename Prec<MIXED>
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const uint32_t g = base + u * nt;
-                if (g >= c1 || !(m[u] & ACTIVE)) continue;
+                if (g >= sw.end || !(m[u] & ACTIVE)) continue;
                 x[g] = xv[u] + alpha * (double)pv[u];
                 const T rn = rv[u] - al * av[u];
                 r[g] = rn;
@@ -576,7 +607,7 @@ __device__ __forceinline__ void u_pass(const Args &a, const typename Prec<MIXED>
     }
 }
 
-template <bool MIXED, int KIND, int NT, int U, int MINB, bool VEC>
+template <bool MIXED, int KIND, int NT, int U, int MINB, bool VEC, int ORD>
 __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
     using T = typename Prec<MIXED>::T;
     mb_ctrl *c = a.ctrl;
@@ -597,7 +628,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
     int red = 0;
 
     double acc[3] = {0.0, 0.0, 0.0}, s3[3];
-    residual_pass<MIXED, KIND, NT, U, VEC>(a, r, bufa, pre, itab, acc);
+    residual_pass<MIXED, KIND, NT, U, VEC, ORD>(a, r, bufa, pre, itab, acc);
     if (!grid_reduce<3, NT>(a, acc, s3, red)) return;
     double rz = s3[0], rr = s3[1];
     double error = s3[2], rr_ref = s3[2];
@@ -611,13 +642,13 @@ __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
         // Q: direction p_new = z + beta p_old fused with A p_new and p.Ap
         T *pcur = first ? pold : pnew;
         double q1[1] = {0.0}, s1[1];
-        q_pass<MIXED, KIND, NT, U, VEC>(a, first, pold, pnew, zb, apb, beta, q1[0]);
+        q_pass<MIXED, KIND, NT, U, VEC, ORD>(a, first, pold, pnew, zb, apb, beta, q1[0]);
         if (!grid_reduce<1, NT>(a, q1, s1, red)) return;
         const double alpha = (pre ? rz : rr) / s1[0];
 
         // U: x += alpha p, r -= alpha A p, z = r / diag
         double u2[2] = {0.0, 0.0}, s2[2];
-        u_pass<MIXED, KIND, NT, U, VEC>(a, pcur, apb, r, zb, pre, itab, alpha, u2);
+        u_pass<MIXED, KIND, NT, U, VEC, ORD>(a, pcur, apb, r, zb, pre, itab, alpha, u2);
         if (!grid_reduce<2, NT>(a, u2, s2, red)) return;
         its += 1;
         pold = pcur;
@@ -637,7 +668,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fcg(Args a) {
             if (s2[1] <= fmax(c->refine_floor, ratio * rr_ref) || its >= max_its) {
                 // FP64 true residual replaces the FP32 recurrence; restart from it
                 double t3[3] = {0.0, 0.0, 0.0};
-                residual_pass<MIXED, KIND, NT, U, VEC>(a, r, pold, pre, itab, t3);
+                residual_pass<MIXED, KIND, NT, U, VEC, ORD>(a, r, pold, pre, itab, t3);
                 if (!grid_reduce<3, NT>(a, t3, s3, red)) return;
                 refinements += 1;
                 error = s3[2];
@@ -748,19 +779,22 @@ struct Variant {
 
 // (threads per block, cells per thread per round, resident blocks per SM,
 // four-cell groups); the group variants need nx to be a multiple of 4
-#define MB_VARIANTS(K)                                                                                          \
-    {(const void *)k_fcg<MIXED, K, 1024, 1, 1, false>, 1024, 0, 1},                                         \
-        {(const void *)k_fcg<MIXED, K, 1024, 1, 2, false>, 1024, 0, 1},                                     \
-        {(const void *)k_fcg<MIXED, K, 512, 2, 2, false>, 512, 0, 2},                                       \
-        {(const void *)k_fcg<MIXED, K, 512, 1, 4, false>, 512, 0, 1},                                       \
-        {(const void *)k_fcg<MIXED, K, 256, 2, 4, false>, 256, 0, 2},                                       \
-        {(const void *)k_fcg<MIXED, K, 1024, 1, 1, true>, 1024, 1, 1},                                      \
-        {(const void *)k_fcg<MIXED, K, 512, 1, 2, true>, 512, 1, 1},                                        \
-        {(const void *)k_fcg<MIXED, K, 256, 1, 4, true>, 256, 1, 1},                                        \
-        {(const void *)k_fcg<MIXED, K, 512, 2, 1, true>, 512, 1, 2},                                        \
-        {(const void *)k_fcg<MIXED, K, 256, 2, 2, true>, 256, 1, 2}
+#define MB_SHAPES(K, O)                                                                                          \
+    {(const void *)k_fcg<MIXED, K, 1024, 1, 1, false, O>, 1024, 0, 1},                                      \
+        {(const void *)k_fcg<MIXED, K, 1024, 1, 2, false, O>, 1024, 0, 1},                                  \
+        {(const void *)k_fcg<MIXED, K, 512, 2, 2, false, O>, 512, 0, 2},                                    \
+        {(const void *)k_fcg<MIXED, K, 512, 1, 4, false, O>, 512, 0, 1},                                    \
+        {(const void *)k_fcg<MIXED, K, 256, 2, 4, false, O>, 256, 0, 2},                                    \
+        {(const void *)k_fcg<MIXED, K, 1024, 1, 1, true, O>, 1024, 1, 1},                                   \
+        {(const void *)k_fcg<MIXED, K, 512, 1, 2, true, O>, 512, 1, 1},                                     \
+        {(const void *)k_fcg<MIXED, K, 256, 1, 4, true, O>, 256, 1, 1},                                     \
+        {(const void *)k_fcg<MIXED, K, 512, 2, 1, true, O>, 512, 1, 2},                                     \
+        {(const void *)k_fcg<MIXED, K, 256, 2, 2, true, O>, 256, 1, 2}
+// variants 0..9: each block sweeps its own range; 10..19: the same shapes
+// with the interleaved sweep
+#define MB_VARIANTS(K) MB_SHAPES(K, 0), MB_SHAPES(K, 1)
 
-constexpr int NUM_VARIANTS = 10;
+constexpr int NUM_VARIANTS = 20;
 
 template <bool MIXED>
 static Variant variant_of(int kind, int v) {
@@ -770,6 +804,7 @@ static Variant variant_of(int kind, int v) {
     return kind == 0 ? t0[v] : (kind == 1 ? t1[v] : t2[v]);
 }
 #undef MB_VARIANTS
+#undef MB_SHAPES
 
 static Variant variant(int mixed, int kind, int v) {
     return mixed ? variant_of<true>(kind, v) : variant_of<false>(kind, v);

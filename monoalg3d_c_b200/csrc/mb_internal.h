@@ -79,6 +79,10 @@ typedef struct mb_stencil_dev {
                                  -x,+x,-y,+y,-z,+z) = that neighbour couples,
                                  bit 6 = the cell is active                 */
     const uint16_t *rowid;    /* kind 2: per cell, k * 9 + class            */
+    uint32_t nzmask;          /* kind 2: bit q = entry q is non-zero in some
+                                 row of the table (bit 13, the diagonal,
+                                 always set); entries whose bit is clear are
+                                 zero in every row and are not read        */
 } mb_stencil_dev;
 
 /* ODE state, device view.  Rows of double (sv64) and float (sv32), each of

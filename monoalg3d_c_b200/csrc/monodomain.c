@@ -652,6 +652,10 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         cudaMemcpy(m->d_table32, t32, tn * sizeof(float), cudaMemcpyHostToDevice);
         free(t32);
         m->st.table = m->d_table; m->st.table32 = m->d_table32;
+        uint32_t nzm = 1u << 13;
+        for (size_t q = 0; q < tn; ++q)
+            if (asmb.table[q] != 0.0) nzm |= 1u << (q % 27);
+        m->st.nzmask = nzm;
     }
     /* per-cell row codes read by the persistent CG */
     if (m->st.kind == 2) {

@@ -19,7 +19,7 @@ import oracle  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-FLAT, RESIDENT = 0, 11          # MB_CG_VARIANT values: flat shape 0, resident kernel (10 flat + tiled before it)
+FLAT, RESIDENT = 0, 21          # MB_CG_VARIANT values: flat shape 0, resident kernel (20 flat + tiled before it)
 
 
 def _stims():

@@ -1,5 +1,6 @@
 """Every launch shape of the persistent CG (one cell per thread, U cells per
-thread, four-cell groups, 2.5D tiles) against the CPU oracle on each
+thread, four-cell groups, each with per-block ranges and interleaved sweeps;
+2.5D tiles) against the CPU oracle on each
 operator kind: constant coefficients with removed cells, per-cell
 conductivity, and the 27-point rows of fibres rotating through the wall.
 The shape the autotuner would pick is forced through MB_CG_VARIANT, which
@@ -46,7 +47,7 @@ def test_every_launch_shape_matches_oracle(case):
     ref = o.v()
     o.close()
     ok = np.isfinite(ref)
-    nv = 11                                      # 10 flat shapes + the tiled kernel
+    nv = 21                                      # 20 flat shapes (two sweep orders) + the tiled kernel
     old = os.environ.get("MB_CG_VARIANT")
     try:
         for v in range(nv):
@@ -79,14 +80,14 @@ def test_every_launch_shape_mixed(case):
     old = os.environ.get("MB_CG_VARIANT")
     its0 = None
     try:
-        for v in range(12):                       # 10 flat shapes, tiled, resident
+        for v in range(22):                       # 20 flat shapes, tiled, resident
             os.environ["MB_CG_VARIANT"] = str(v)
             t = Tissue(nx, ny, nz, precision="mixed", stims=stims, **kw)
             kernel = t.tuning()["cg_kernel"]
-            if v == 11 and kernel != 200:
+            if v == 21 and kernel != 200:
                 t.close()                         # the resident kernel does not apply to this operator
                 continue
-            assert kernel == {10: 100, 11: 200}.get(v, v), f"variant {v} not used ({kernel})"
+            assert kernel == {20: 100, 21: 200}.get(v, v), f"variant {v} not used ({kernel})"
             t.step(STEPS)
             got = t.v()
             its = t.step_stats(0, STEPS)["its"]
