@@ -327,7 +327,7 @@ def main():
     achieved = b / (dur * 1e-3) / 1e9
     traffic = None
     if name.startswith("k_pcg"):
-        traffic = PROFILED_TRAFFIC.get((wl.name, "groups" if 5 <= cg_kernel < 10 else cg_kernel))
+        traffic = PROFILED_TRAFFIC.get((wl.name, "groups" if cg_kernel == 5 else cg_kernel))
     roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
             "bytes_per_launch": b,

@@ -355,12 +355,15 @@ int mb_monodomain_time_steps_host_async(mb_monodomain *m, int n, const double *s
 /* Launch choices made at creation by timing: the ODE kernel's variant
  * (0..5 = one-cell-per-thread launches with at least 1..6 resident 128-thread
  * blocks per SM, 6..9 = staged persistent launches with at least 1..4), the
- * CG grid size and the CG kernel (-1 = graph of separate kernels, 0..19 =
- * launch shape of the flat persistent kernel -- 0..9 with a contiguous range
- * of cells per block, 10..19 the same shapes sweeping the grid interleaved --,
- * 100 = the 2.5D tiled persistent kernel, 200 = the resident tile-column
- * kernel). */
+ * CG grid size and the CG kernel (-1 = graph of separate kernels, 0..n-1 =
+ * launch shape of the flat persistent kernel, n = mb_cg_launch_shapes --
+ * the first half with a contiguous range of cells per block, the second the
+ * same shapes sweeping the grid interleaved --, 100 = the 2.5D tiled
+ * persistent kernel, 200 = the resident tile-column kernel).  The
+ * environment variable MB_CG_VARIANT, read at creation, forces a choice:
+ * 0..n-1 a flat shape, n the tiled kernel, n + 1 the resident kernel. */
 int mb_monodomain_tuning(mb_monodomain *m, int *ode_variant, int *cg_blocks, int *cg_kernel);
+int mb_cg_launch_shapes(int *flat_shapes);
 
 /* ---- general sparse CG (test_solvers.c fixtures) ---------------------- */
 /* Solves A x = b for a CSR matrix on the device; x holds the initial guess

@@ -52,7 +52,7 @@ EXPORTED = [
     "mb_monodomain_get_state", "mb_monodomain_info", "mb_monodomain_step_stats",
     "mb_monodomain_device_v", "mb_monodomain_profile_steps", "mb_csr_conjugate_gradient",
     "mb_monodomain_tuning", "mb_monodomain_time_steps", "mb_monodomain_time_steps_host",
-    "mb_csr_conjugate_gradient_noalloc",
+    "mb_csr_conjugate_gradient_noalloc", "mb_cg_launch_shapes",
 ]
 
 
@@ -172,6 +172,7 @@ def _load() -> C.CDLL:
         "mb_csr_solve": (i32, [vp, vp, vp, dbl, i32, i32, P(u32), P(dbl)]),
         "mb_csr_destroy": (None, [vp]),
         "mb_monodomain_tuning": (i32, [vp, P(i32), P(i32), P(i32)]),
+        "mb_cg_launch_shapes": (i32, [P(i32)]),
         "mb_monodomain_time_steps": (i32, [vp, i32, P(dbl)]),
         "mb_monodomain_time_steps_host": (i32, [vp, i32, vp, vp, P(dbl)]),
         "mb_csr_conjugate_gradient_noalloc": (i32, [i32, vp, vp, vp, vp, vp, dbl, i32, i32, P(u32), P(dbl), vp]),

@@ -294,15 +294,43 @@ struct Direction {
     __device__ __forceinline__ T at(uint32_t i) const { return z[i] + beta * p[i]; }
 };
 
+// The values left of a stencil row's first cell and right of its last.  The
+// lanes of a warp hold consecutive groups, so where the lane below holds the
+// group g0 - 4 of the same x-row (lc), its row for the same (dz, dy) starts
+// at b - 4 (rows of one x-row are clamped alike) and the value left of this
+// row is the last one it read: it comes by shuffle, and likewise from the
+// lane above (rc).  Other lanes (lane 0 and 31, groups on an x face, lanes
+// past the end of a range) load it, with a load whose condition is known
+// before the row's loads.  The same values as loading every one of them,
+// without the 16-byte-strided scalar loads.  All 32 lanes call it together.
+template <typename T, typename F>
+__device__ __forceinline__ void x_sides(const F &f, bool lc, bool rc, uint32_t b, uint32_t n, const Vec4<T> &mid,
+                                        bool need_l, bool need_r, T &wl, T &wr) {
+    T l = T(0), r = T(0);
+    if (need_l && !lc) l = f.at(b > 0 ? b - 1 : b);
+    if (need_r && !rc) r = f.at(b + 4 < n ? b + 4 : b);
+    const T sl = __shfl_up_sync(0xffffffffu, mid.v[3], 1);
+    const T sr = __shfl_down_sync(0xffffffffu, mid.v[0], 1);
+    wl = lc ? sl : l;
+    wr = rc ? sr : r;
+}
+
 // (A f) for the group at g0: pc = f at the 4 cells, ap = the products, m =
-// the cells' code bytes (kind 2: all active).
+// the cells' code bytes (kind 2: all active).  All 32 lanes call it together.
 template <typename T, int KIND, typename F>
 __device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, const F &f, Vec4<T> &pc, Vec4<T> &ap,
                                        unsigned (&m)[4]) {
     const uint32_t sy = (uint32_t)st.nx, sz = (uint32_t)st.nx * (uint32_t)st.ny, n = sz * (uint32_t)st.nz;
     pc = f.row(g0);
     if constexpr (KIND == 2) {
+        const unsigned lane = threadIdx.x & 31u;
+        const uint32_t gl = __shfl_up_sync(0xffffffffu, g0, 1), gr = __shfl_down_sync(0xffffffffu, g0, 1);
+        // the lane below / above holds the adjacent group of the same x-row
+        bool lc = lane != 0u && gl + 4u == g0, rc = lane != 31u && gr == g0 + 4u;
         const ushort4 rid = *reinterpret_cast<const ushort4 *>(st.rowid + g0);
+        // x class of the first / last cell (row id = k 9 + y class 3 + x class)
+        lc = lc && (rid.x % 3u) != 0u;
+        rc = rc && (rid.w % 3u) != 2u;
         const size_t rw[4] = {(size_t)rid.x * 27, (size_t)rid.y * 27, (size_t)rid.z * 27, (size_t)rid.w * 27};
         // away from the x faces the four cells share one table row
         const bool uni = rid.x == rid.y && rid.x == rid.z && rid.x == rid.w;
@@ -322,10 +350,9 @@ __device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, co
                 if (dy > 0) b = b + sy < n ? b + sy : g0;
                 const Vec4<T> mid = (dz == 0 && dy == 0) ? pc : f.row(b);
                 T w[6];
-                w[0] = (rb & 1u) ? f.at(b > 0 ? b - 1 : b) : T(0);
+                x_sides<T>(f, lc, rc, b, n, mid, (rb & 1u) != 0u, (rb & 4u) != 0u, w[0], w[5]);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) w[k + 1] = mid.v[k];
-                w[5] = (rb & 4u) ? f.at(b + 4 < n ? b + 4 : b) : T(0);
 #pragma unroll
                 for (int dx = -1; dx <= 1; ++dx) {
                     if (!((rb >> (dx + 1)) & 1u)) continue;
@@ -347,6 +374,8 @@ __device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, co
     } else {
         const uchar4 cd = *reinterpret_cast<const uchar4 *>(st.code + g0);
         m[0] = cd.x; m[1] = cd.y; m[2] = cd.z; m[3] = cd.w;
+        // two values per group: plain loads (the shuffles' bookkeeping costs
+        // registers these forms do not have to spare)
         const T xl = f.at(g0 > 0 ? g0 - 1 : g0), xr = f.at(g0 + 4 < n ? g0 + 4 : g0);
         const Vec4<T> ym = f.row(g0 >= sy ? g0 - sy : g0), yp = f.row(g0 + sy < n ? g0 + sy : g0);
         const Vec4<T> zm = f.row(g0 >= sz ? g0 - sz : g0), zp = f.row(g0 + sz < n ? g0 + sz : g0);
@@ -391,15 +420,19 @@ __device__ __forceinline__ void apply4(const mb_stencil_dev &st, uint32_t g0, co
 template <typename T, int KIND, int NT, int U, int ORD, typename F, typename ACT>
 __device__ __forceinline__ void pass4(const mb_stencil_dev &st, const F &f, ACT act) {
     const uint32_t groups = ((uint32_t)st.nx * st.ny * st.nz) >> 2;
-    const uint32_t nt = blockDim.x;     // <= NT: the host sizes blocks to whole rounds
+    const uint32_t nt = blockDim.x;     // <= NT, a multiple of 32: the host sizes blocks to whole rounds
+    const uint32_t lane = threadIdx.x & 31u;
     const Sweep<ORD> sw(groups, U * nt);
-    for (uint32_t q = sw.start; q < sw.end; q += sw.step) {
+    // a warp runs its rounds together (while its first lane's unit is in
+    // range; lanes past the end repeat the range's last group and skip act),
+    // as apply4's shuffles need
+    for (uint32_t q = sw.start; q - lane < sw.end; q += sw.step) {
         Vec4<T> pc[U], ap[U];
         unsigned m[U][4];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t qq = q + u * nt;
-            apply4<T, KIND>(st, (qq < sw.end ? qq : q) << 2, f, pc[u], ap[u], m[u]);
+            apply4<T, KIND>(st, (qq < sw.end ? qq : sw.end - 1u) << 2, f, pc[u], ap[u], m[u]);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
@@ -789,12 +822,15 @@ struct Variant {
         {(const void *)k_fcg<MIXED, K, 512, 1, 2, true, O>, 512, 1, 1},                                     \
         {(const void *)k_fcg<MIXED, K, 256, 1, 4, true, O>, 256, 1, 1},                                     \
         {(const void *)k_fcg<MIXED, K, 512, 2, 1, true, O>, 512, 1, 2},                                     \
-        {(const void *)k_fcg<MIXED, K, 256, 2, 2, true, O>, 256, 1, 2}
-// variants 0..9: each block sweeps its own range; 10..19: the same shapes
-// with the interleaved sweep
+        {(const void *)k_fcg<MIXED, K, 256, 2, 2, true, O>, 256, 1, 2},                                     \
+        {(const void *)k_fcg<MIXED, K, 512, 1, 1, true, O>, 512, 1, 1},                                     \
+        {(const void *)k_fcg<MIXED, K, 256, 1, 2, true, O>, 256, 1, 1}
+// variants 0..11: each block sweeps its own range; 12..23: the same shapes
+// with the interleaved sweep.  The last two shapes give a thread 128
+// registers, enough for every row load of a 27-point group in flight.
 #define MB_VARIANTS(K) MB_SHAPES(K, 0), MB_SHAPES(K, 1)
 
-constexpr int NUM_VARIANTS = 20;
+constexpr int NUM_VARIANTS = 24;
 
 template <bool MIXED>
 static Variant variant_of(int kind, int v) {

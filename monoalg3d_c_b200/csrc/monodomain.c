@@ -926,6 +926,12 @@ static int ode_autotune(mb_monodomain *m) {
     return rc;
 }
 
+int mb_cg_launch_shapes(int *flat_shapes) {
+    if (!flat_shapes) return set_err(MB_ERR_ARG, "null");
+    *flat_shapes = mbk_fcg_variants(0);
+    return MB_OK;
+}
+
 int mb_monodomain_tuning(mb_monodomain *m, int *ode_variant, int *cg_blocks, int *cg_kernel) {
     if (!m) return set_err(MB_ERR_ARG, "null");
     if (ode_variant) *ode_variant = m->ode.variant;

@@ -333,6 +333,14 @@ class Tissue:
         return {"ode_ms": a.value, "cg_ms": b.value, "step_ms": c.value, "cg_iterations": it.value}
 
 
+def cg_launch_shapes() -> int:
+    """Number of launch shapes of the flat persistent CG (MB_CG_VARIANT values
+    0..n-1; n selects the tiled kernel, n + 1 the resident one)."""
+    n = C.c_int()
+    check(lib.mb_cg_launch_shapes(C.byref(n)))
+    return n.value
+
+
 class OdeSolver:
     """GPU cell-model library for independent cells (set_model_initial_conditions_gpu /
     solve_model_odes_gpu, ode_solver.h:37-47)."""

@@ -19,7 +19,13 @@ import oracle  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-FLAT, RESIDENT = 0, 21          # MB_CG_VARIANT values: flat shape 0, resident kernel (20 flat + tiled before it)
+FLAT = 0                        # MB_CG_VARIANT of flat shape 0
+
+
+def _resident():
+    """MB_CG_VARIANT of the resident kernel (after the flat shapes and the tiled kernel)."""
+    from monoalg3d_c_b200.monodomain import cg_launch_shapes
+    return cg_launch_shapes() + 1
 
 
 def _stims():
@@ -69,7 +75,7 @@ def _kw(name, n, seed=5):
 def test_resident_matches_flat_and_oracle(case):
     nx, ny, nz, steps, kind = CASES[case]
     kw = _kw(kind, nx * ny * nz)
-    k_res, v_res, s_res = _run(nx, ny, nz, steps, RESIDENT, **kw)
+    k_res, v_res, s_res = _run(nx, ny, nz, steps, _resident(), **kw)
     assert k_res == 200, f"resident kernel not used ({k_res})"
     k_flat, v_flat, s_flat = _run(nx, ny, nz, steps, FLAT, **kw)
     assert k_flat == 0

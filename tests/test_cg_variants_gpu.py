@@ -47,7 +47,8 @@ def test_every_launch_shape_matches_oracle(case):
     ref = o.v()
     o.close()
     ok = np.isfinite(ref)
-    nv = 21                                      # 20 flat shapes (two sweep orders) + the tiled kernel
+    from monoalg3d_c_b200.monodomain import cg_launch_shapes
+    nv = cg_launch_shapes() + 1                  # flat shapes (two sweep orders) + the tiled kernel
     old = os.environ.get("MB_CG_VARIANT")
     try:
         for v in range(nv):
@@ -77,17 +78,19 @@ def test_every_launch_shape_mixed(case):
     ref = o.v()
     o.close()
     ok = np.isfinite(ref)
+    from monoalg3d_c_b200.monodomain import cg_launch_shapes
+    nf = cg_launch_shapes()
     old = os.environ.get("MB_CG_VARIANT")
     its0 = None
     try:
-        for v in range(22):                       # 20 flat shapes, tiled, resident
+        for v in range(nf + 2):                   # flat shapes, tiled, resident
             os.environ["MB_CG_VARIANT"] = str(v)
             t = Tissue(nx, ny, nz, precision="mixed", stims=stims, **kw)
             kernel = t.tuning()["cg_kernel"]
-            if v == 21 and kernel != 200:
+            if v == nf + 1 and kernel != 200:
                 t.close()                         # the resident kernel does not apply to this operator
                 continue
-            assert kernel == {20: 100, 21: 200}.get(v, v), f"variant {v} not used ({kernel})"
+            assert kernel == {nf: 100, nf + 1: 200}.get(v, v), f"variant {v} not used ({kernel})"
             t.step(STEPS)
             got = t.v()
             its = t.step_stats(0, STEPS)["its"]
