@@ -139,11 +139,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-# DRAM bytes per launch of the dominant kernel, from one ncu capture of the same
-# workload (profiles/k_fcg_group_mixed_slab_200x200x50.md; the four-cell-group
-# launch shape, whose variants read and write the same data):
-# dram__bytes_read.sum + dram__bytes_write.sum.
-PROFILED_TRAFFIC = {("slab_200x200x50_torord_fibrosis20", "groups"): 177.3e6}
+# DRAM bytes per launch of the dominant kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum), keyed by workload and CG launch shape:
+#   - from one ncu capture of the same workload and shape
+#     (profiles/k_fcg_group_mixed_slab_200x200x50.md);
+#   - per active cell and CG iteration, from a capture of a smaller case of
+#     the same workload and shape (360x360x72, inputs larger than L2; the
+#     interleaved sweep's traffic grows with the cells), scaled by the
+#     launch's cells and iterations (profiles/k_fcg_group_mixed_slab_500x500x100.md).
+PROFILED_TRAFFIC = {("slab_200x200x50_torord_fibrosis20", 5): 177.3e6}
+PROFILED_TRAFFIC_PER_CELL_ITERATION = {("slab_500x500x100_torord_rotating_fibres", 17): 58.83}
 
 
 def measured_hbm():
@@ -325,14 +330,19 @@ def main():
     else:
         name, b, dur = f"k_{model}_mixed (Rush-Larsen ODE)", od_b, prof_mx["ode_ms"]
     achieved = b / (dur * 1e-3) / 1e9
-    traffic = None
+    traffic, note = None, "algorithmic bytes / CUDA-event time"
     if name.startswith("k_pcg"):
-        traffic = PROFILED_TRAFFIC.get((wl.name, "groups" if cg_kernel == 5 else cg_kernel))
+        traffic = PROFILED_TRAFFIC.get((wl.name, cg_kernel))
+        if traffic is not None:
+            note += "; traffic = DRAM bytes per launch measured by ncu (the solve's working set stays in L2)"
+        per = PROFILED_TRAFFIC_PER_CELL_ITERATION.get((wl.name, cg_kernel))
+        if per is not None:
+            traffic = per * n_active * its
+            note += ("; traffic = DRAM bytes per cell-iteration measured by ncu on a 360x360x72 case of the "
+                     "same kernel, times the launch's cells and iterations")
     roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
-            "bytes_per_launch": b,
-            "note": "algorithmic bytes / CUDA-event time; the CG working set stays in L2 on this workload "
-                    "(traffic = DRAM bytes per launch measured by ncu)"}
+            "bytes_per_launch": b, "note": note}
 
     out = {
         "metric": metric, "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps,
