@@ -147,10 +147,14 @@ class ClockSampler:
 #     the same workload and shape (360x360x72, inputs larger than L2; the
 #     interleaved sweep's traffic grows with the cells), scaled by the
 #     launch's cells and iterations (profiles/k_fcg_group_mixed_slab_500x500x100.md).
-# Keys: (workload, ("groups", sweep order)) -- every four-cell-group launch shape
-# of one sweep order reads and writes the same data.
-PROFILED_TRAFFIC = {("slab_200x200x50_torord_fibrosis20", ("groups", 0)): 177.3e6}
-PROFILED_TRAFFIC_PER_CELL_ITERATION = {("slab_500x500x100_torord_rotating_fibres", ("groups", 1)): 58.83}
+# Keys: (workload, launch shape), else (workload, ("groups", sweep order)) --
+# the four-cell-group shapes of one sweep order read and write the same data,
+# so their DRAM traffic differs only by what L2 keeps between passes.
+PROFILED_TRAFFIC = {("slab_200x200x50_torord_fibrosis20", 10): 145.5e6,
+                    ("slab_200x200x50_torord_fibrosis20", 5): 177.3e6,
+                    ("slab_200x200x50_torord_fibrosis20", ("groups", 0)): 177.3e6}
+PROFILED_TRAFFIC_PER_CELL_ITERATION = {("slab_500x500x100_torord_rotating_fibres", 17): 58.83,
+                                       ("slab_500x500x100_torord_rotating_fibres", ("groups", 1)): 58.83}
 FLAT_SHAPES_PER_ORDER = 12     # flat CG shapes per sweep order; the last 7 of each run four-cell groups
 
 
@@ -341,10 +345,11 @@ def main():
     achieved = b / (dur * 1e-3) / 1e9
     traffic, note = None, "algorithmic bytes / CUDA-event time"
     if name.startswith("k_pcg"):
-        traffic = PROFILED_TRAFFIC.get((wl.name, traffic_key(cg_kernel)))
+        traffic = PROFILED_TRAFFIC.get((wl.name, cg_kernel), PROFILED_TRAFFIC.get((wl.name, traffic_key(cg_kernel))))
         if traffic is not None:
             note += "; traffic = DRAM bytes per launch measured by ncu (the solve's working set stays in L2)"
-        per = PROFILED_TRAFFIC_PER_CELL_ITERATION.get((wl.name, traffic_key(cg_kernel)))
+        per = PROFILED_TRAFFIC_PER_CELL_ITERATION.get(
+            (wl.name, cg_kernel), PROFILED_TRAFFIC_PER_CELL_ITERATION.get((wl.name, traffic_key(cg_kernel))))
         if per is not None:
             traffic = per * n_active * its
             note += ("; traffic = DRAM bytes per cell-iteration measured by ncu on a 360x360x72 case of the "
