@@ -30,7 +30,7 @@ LIBS = os.path.join(REF, "shared_libs")
 
 # Each case: geometry (cells), model, assembly and simulation length.
 CASES = {
-    # configs[0]'s method on a small cuboid: TT2006, homogeneous sigma, Jacobi PCG 1e-16
+    # the plain FP64 method on a small cuboid: TT2006, homogeneous sigma, Jacobi PCG 1e-16
     "tt2006_cuboid": dict(nx=32, ny=8, nz=2, model="tt2006", assembly="homogeneous", sim_ms=12.0),
     # ToRORd-fkatp endo/mid/epi library, no extra data (every cell ENDO)
     "torord_endo_cuboid": dict(nx=32, ny=8, nz=2, model="torord", assembly="homogeneous", sim_ms=12.0),
