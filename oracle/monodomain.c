@@ -74,6 +74,12 @@ static double stim_value(const mb_stim *st, int nx, int ny, int64_t g, double dx
     return on ? st->current : 0.0;
 }
 
+void orc_stim_values(const mb_monodomain_desc *d, const int32_t *cells, int32_t n, double *out) {
+    for (int k = 0; k < d->num_stims; ++k)
+        for (int32_t c = 0; c < n; ++c)
+            out[(size_t)k * n + c] = stim_value(&d->stims[k], d->nx, d->ny, cells[c], d->dx, d->dy, d->dz);
+}
+
 int orc_create(orc_sim **out, const mb_monodomain_desc *d) {
     if (!out || !d || d->nx <= 0 || d->ny <= 0 || d->nz <= 0 || d->num_stims < 0 || d->num_stims > MB_MAX_STIMS)
         return MB_ERR_ARG;

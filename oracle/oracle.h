@@ -84,6 +84,25 @@ int32_t orc_active_cells(const orc_sim *s);
 void orc_destroy(orc_sim *s);
 /* Loop steps the reference takes for final time T (cur_time - T <= dt). */
 int orc_loop_steps(double final_time, double dt);
+/* Per-row stimulus values of every stimulus (num_stims x n), for the rows
+ * whose grid indices are cells[] (stimuli.c:56-91,426-520). */
+void orc_stim_values(const mb_monodomain_desc *d, const int32_t *cells, int32_t n, double *out);
+
+/* ---- tangent-linear loop (tangent.cc) ----------------------------------- */
+
+/* Runs nsteps loop steps of a TT2006 tissue with per-cell conductivity
+ * (MB_ASSEMBLY_PER_CELL_SIGMA) and samples V at the sensor cells (grid
+ * indices) after every sample_every steps.  Returns the L2 misfit
+ * loss = 1/2 sum (sample - target)^2 (target: nsteps / sample_every rows of
+ * n_sensors) and its derivative dloss along the direction (dsigma, dgkr):
+ * per grid cell, a change of the conductivity and of the gKr scaling (either
+ * may be NULL).  Forward mode: the cell model runs orc_tt2006_step's
+ * statements on dual numbers, and every implicit solve A v = b is followed by
+ * the tangent solve A dv = alpha dV* - dA v, dA from the derivative of the
+ * harmonic-mean face conductivities.  Returns 0 or an MB_ERR_* code. */
+int orc_tangent_misfit(const mb_monodomain_desc *d, int nsteps, int sample_every, int n_sensors,
+                       const int64_t *sensors, const double *target, const double *dsigma, const double *dgkr,
+                       double *loss, double *dloss);
 
 #ifdef __cplusplus
 }

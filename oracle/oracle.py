@@ -47,6 +47,7 @@ def load() -> C.CDLL:
     lib.orc_assemble.argtypes = [vp, vp, vp]
     lib.orc_csr_free.argtypes = [vp]
     lib.orc_pcg.argtypes = [vp, vp, vp, C.c_double, C.c_int, C.c_int, u32p, dp]
+    lib.orc_tangent_misfit.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, dp, dp]
     _lib = lib
     return lib
 
@@ -147,6 +148,29 @@ def pcg(row_ptr, col, val, b, x0, tol=1e-16, max_its=200, use_preconditioner=Tru
     lib.orc_pcg(C.byref(A), _p(bb), _p(x), tol, int(max_its), 1 if use_preconditioner else 0, C.byref(its),
                 C.byref(err))
     return x, its.value, err.value
+
+
+def tangent_misfit(nx: int, ny: int, nz: int, steps: int, sample_every: int, sensors, target,
+                   dsigma: Optional[np.ndarray] = None, dgkr: Optional[np.ndarray] = None, **kw):
+    """The loop's L2 misfit 1/2 sum (V at the sensors after every sample_every
+    steps - target)^2 and its exact directional derivative along (dsigma,
+    dgkr) (per grid cell), from the tangent-linear loop (tangent.cc).
+    Returns (loss, dloss)."""
+    lib = load()
+    kw = dict(kw)
+    kw.pop("precision", None)
+    d, keep = _desc(nx, ny, nz, **kw)
+    sens = np.ascontiguousarray(sensors, dtype=np.int64)
+    tgt = np.ascontiguousarray(target, dtype=np.float64)
+    ds = None if dsigma is None else np.ascontiguousarray(dsigma, dtype=np.float64)
+    dg = None if dgkr is None else np.ascontiguousarray(dgkr, dtype=np.float64)
+    loss, dloss = C.c_double(), C.c_double()
+    rc = lib.orc_tangent_misfit(C.byref(d), int(steps), int(sample_every), int(sens.size), _p(sens), _p(tgt),
+                                _p(ds), _p(dg), C.byref(loss), C.byref(dloss))
+    del keep
+    if rc != 0:
+        raise RuntimeError(f"orc_tangent_misfit failed ({rc})")
+    return loss.value, dloss.value
 
 
 def tt2006_initial_state() -> np.ndarray:

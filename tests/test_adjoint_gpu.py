@@ -1,10 +1,12 @@
 """Discrete adjoint of the loop (mb_adjoint_*): gradients of an L2 misfit of V
 at sensor cells with respect to the per-cell conductivity and gKr scaling,
 against central finite differences of the same FP64 GPU loop along random
-directions, against central differences of the CPU oracle (FP64), and through
-the torch.autograd.Function.
+directions, against central differences of the CPU oracle (FP64), against
+the oracle's FP64 tangent-linear loop (exact directional derivatives), and
+through the torch.autograd.Function.
 
-Bar: directional derivatives within 1e-4 relative of the finite differences.
+Bar: directional derivatives within 1e-4 relative of the finite differences,
+within 1e-6 relative of the tangent-linear derivatives.
 The loop's CG tolerance is tightened to 1e-24 so that the solves' own error
 does not dominate the differences; the gKr scaling is applied as a float, so
 its differences use the float-rounded perturbed values."""
@@ -105,6 +107,29 @@ def test_gradients_match_cpu_oracle_differences():
           loss(_oracle_traces(nx, ny, steps, sigma, km, sensors, 50))) / 2.0
     ad = np.sum(gk * (kp - km)) / 2.0
     assert abs(ad - fd) <= REL * abs(fd) + 1e-12, f"gKr: adjoint {ad:.10e}, oracle fd {fd:.10e}"
+
+
+def test_gradients_match_cpu_tangent_linear():
+    from monoalg3d_c_b200.adjoint import Adjoint
+    nx, ny, steps, sigma, gkr, sensors = _problem(10, 8, 300, seed=3)
+    adj = Adjoint(nx, ny, 1, sigma, gkr, sensors, nsteps=steps, sample_every=50, checkpoint_every=40, **_kw())
+    target = _oracle_traces(nx, ny, steps, sigma * 0.8, gkr, sensors, 50)
+    tr = adj.forward(sigma, gkr)
+    gs, gk = adj.backward(tr - target)
+    adj.close()
+    sc = np.ones((5, nx * ny))
+    sc[1] = gkr
+    tl = dict(assembly="per_cell", sigma_cell=sigma, current_scale=sc, **_kw())
+    rng = np.random.default_rng(11)
+    for trial in range(2):
+        d = rng.standard_normal(sigma.size)
+        _, tl_d = oracle.tangent_misfit(nx, ny, 1, steps, 50, sensors, target, dsigma=sigma * d, **tl)
+        ad = np.sum(gs * sigma * d)
+        assert abs(ad - tl_d) <= 1e-6 * abs(tl_d), f"sigma {trial}: adjoint {ad:.12e}, tangent {tl_d:.12e}"
+        dg = rng.standard_normal(gkr.size)
+        _, tl_g = oracle.tangent_misfit(nx, ny, 1, steps, 50, sensors, target, dgkr=gkr * dg, **tl)
+        ad = np.sum(gk * gkr * dg)
+        assert abs(ad - tl_g) <= 1e-6 * abs(tl_g), f"gKr {trial}: adjoint {ad:.12e}, tangent {tl_g:.12e}"
 
 
 def test_autograd_function():

@@ -116,3 +116,60 @@ def test_ecg_restatement_matches_reference():
         checked += 1
     assert checked >= 20
     assert np.abs(g["ecg"]).max() > 0.5        # the wave's signal, not only zeros
+
+
+def _tangent_problem():
+    from monoalg3d_c_b200 import Stim
+    nx, ny, steps, every = 10, 8, 300, 50
+    rng = np.random.default_rng(3)
+    n = nx * ny
+    sigma = 0.00013 * np.exp(0.3 * rng.standard_normal(n))
+    gkr = np.exp(0.2 * rng.standard_normal(n))
+    sensors = rng.choice(n, size=6, replace=False)
+    kw = dict(stims=[Stim(kind="x_less_than", start=0.0, duration=2.0, current=-53.0, x_limit=500.0)],
+              cg_tolerance=1e-24, cg_max_iterations=500, assembly="per_cell")
+    return nx, ny, steps, every, sigma, gkr, sensors, kw, rng
+
+
+def _scales(gkr):
+    sc = np.ones((5, gkr.size))
+    sc[1] = gkr
+    return sc
+
+
+def _oracle_misfit(nx, ny, steps, every, sigma, gkr, sensors, kw, target):
+    o = oracle.Sim(nx, ny, 1, sigma_cell=sigma, current_scale=_scales(gkr), **kw)
+    tr = []
+    for _ in range(steps // every):
+        o.step(every)
+        tr.append(o.v()[sensors])
+    o.close()
+    tr = np.array(tr)
+    return tr, 0.5 * float(np.sum((tr - target) ** 2))
+
+
+def test_tangent_linear_loop_matches_oracle_differences():
+    """The tangent-linear loop (tangent.cc) against central differences of the
+    oracle loop: its misfit equals the loop's, and its directional derivatives
+    along a conductivity and a gKr direction agree to 1e-6 relative (the
+    differences' own truncation error: h^2 ~ 1e-8 for the conductivity; the gKr
+    scaling is applied as a float, so its differences use the rounded values)."""
+    nx, ny, steps, every, sigma, gkr, sensors, kw, rng = _tangent_problem()
+    target, _ = _oracle_misfit(nx, ny, steps, every, sigma * 0.8, gkr, sensors, kw, 0.0)
+    _, loss = _oracle_misfit(nx, ny, steps, every, sigma, gkr, sensors, kw, target)
+    d = rng.standard_normal(sigma.size)
+    tl_loss, tl_d = oracle.tangent_misfit(nx, ny, 1, steps, every, sensors, target, dsigma=sigma * d,
+                                          sigma_cell=sigma, current_scale=_scales(gkr), **kw)
+    assert abs(tl_loss - loss) <= 1e-12 * abs(loss)
+    h = 1e-4
+    fd = (_oracle_misfit(nx, ny, steps, every, sigma * (1 + h * d), gkr, sensors, kw, target)[1] -
+          _oracle_misfit(nx, ny, steps, every, sigma * (1 - h * d), gkr, sensors, kw, target)[1]) / (2 * h)
+    assert abs(tl_d - fd) <= 1e-6 * abs(fd), f"sigma: tangent {tl_d:.12e}, differences {fd:.12e}"
+    dg = rng.standard_normal(gkr.size)
+    kp = np.float32(gkr * (1 + 1e-3 * dg)).astype(np.float64)
+    km = np.float32(gkr * (1 - 1e-3 * dg)).astype(np.float64)
+    fd = (_oracle_misfit(nx, ny, steps, every, sigma, kp, sensors, kw, target)[1] -
+          _oracle_misfit(nx, ny, steps, every, sigma, km, sensors, kw, target)[1]) / 2.0
+    _, tl_g = oracle.tangent_misfit(nx, ny, 1, steps, every, sensors, target, dgkr=(kp - km) / 2.0,
+                                    sigma_cell=sigma, current_scale=_scales(gkr), **kw)
+    assert abs(tl_g - fd) <= 1e-6 * abs(fd), f"gKr: tangent {tl_g:.12e}, differences {fd:.12e}"
