@@ -188,6 +188,26 @@ def cg_bytes(prec: str, n_active: int, n_grid: int, its: float, refinements: flo
     return n_active * (32.0 * its + 24.0 * max(refinements, 1.0)) + mask
 
 
+def activation_error(wl, steps: int) -> dict:
+    """Untimed: the workload in both precisions with activation (-30 mV)
+    tracked on the device, first activation times compared after `steps`
+    steps over the cells activated in both runs."""
+    first = {}
+    for prec in ("mixed", "fp64"):
+        t = wl.tissue(precision=prec, track_activation=True)
+        t.step(steps)
+        t.sync()
+        first[prec] = t.activation()["first"].astype(np.float64)
+        t.close()
+    a, b = first["mixed"], first["fp64"]
+    both = (a >= 0) & (b >= 0)
+    d = a[both] - b[both]
+    return {"after_steps": steps, "cells_activated": int(both.sum()),
+            "activated_in_one_run_only": int(((a >= 0) != (b >= 0)).sum()),
+            "max_ms": float(np.abs(d).max()) if d.size else None,
+            "rms_ms": float(np.sqrt(np.mean(d * d))) if d.size else None}
+
+
 def ode_bytes(model: str, prec: str, n_active: int) -> float:
     """State read + written once per cell-step, plus V in and V* out."""
     per = {("tt2006", "fp64"): 18 * 8, ("tt2006", "mixed"): 5 * 8 + 13 * 4,
@@ -323,6 +343,12 @@ def main():
     tune = t_mx.tuning()
     t_mx_tuning = tune
     t_mx.close()
+    # activation-time error of the mixed form (untimed, rank 0; 40 ms of the
+    # workload; the 25 M-cell slab is left to the accuracy check module)
+    if rank == 0 and wl.n <= 4_000_000:
+        act_err = activation_error(wl, 2000)
+    else:
+        act_err = {"skipped": "run python -m monoalg3d_c_b200.accuracy_check for this workload"}
 
     cell_steps = n_active * args.steps * ws
     value = cell_steps / (ms_mx * 1e-3)
@@ -375,7 +401,7 @@ def main():
                   "fp64_residual_evaluations_per_step": refs, "ode_variant": tune["ode_variant"],
                   "cg_blocks": tune["cg_blocks"], "cg_kernel": tune["cg_kernel"]},
         "error_vs_fp64": {"v_rms_mv": float(np.sqrt(np.mean(dv ** 2))), "v_max_mv": float(np.max(np.abs(dv))),
-                          "after_steps": args.warmup + args.steps + 3},
+                          "after_steps": args.warmup + args.steps + 3, "activation_ms": act_err},
         "roofline": roof,
         "kernels": {"ode_mixed": {"ms": prof_mx["ode_ms"], "bytes": od_b,
                                   "GBps": od_b / (prof_mx["ode_ms"] * 1e-3) / 1e9},
