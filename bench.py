@@ -155,6 +155,11 @@ PROFILED_TRAFFIC = {("slab_200x200x50_torord_fibrosis20", 10): 145.5e6,
                     ("slab_200x200x50_torord_fibrosis20", ("groups", 0)): 177.3e6}
 PROFILED_TRAFFIC_PER_CELL_ITERATION = {("slab_500x500x100_torord_rotating_fibres", 17): 58.83,
                                        ("slab_500x500x100_torord_rotating_fibres", ("groups", 1)): 58.83}
+# Pipe utilisation of the mixed ODE kernel from one ncu capture of the same
+# workload (profiles/k_torord_mixed_slab_200x200x50.md): XU = the MUFU pipe
+# (ex2, lg2, rcp, rsqrt: the exp/log/divide-bound part), FMA = the FP32 pipe.
+PROFILED_ODE_PIPES = {"slab_200x200x50_torord_fibrosis20": {"xu_pct": 46.8, "fma_pct": 32.8, "fp64_pct": 1.1,
+                                                            "issue_active_pct": 53.7}}
 FLAT_SHAPES_PER_ORDER = 12     # flat CG shapes per sweep order; the last 7 of each run four-cell groups
 
 
@@ -403,6 +408,10 @@ def main():
         "error_vs_fp64": {"v_rms_mv": float(np.sqrt(np.mean(dv ** 2))), "v_max_mv": float(np.max(np.abs(dv))),
                           "after_steps": args.warmup + args.steps + 3, "activation_ms": act_err},
         "roofline": roof,
+        "ode_roofline": {"kernel": f"k_{model}_mixed (Rush-Larsen ODE)", "bound": "sfu/fp32 (MUFU) and hbm",
+                         "achieved_hbm": od_b / (prof_mx["ode_ms"] * 1e-3) / 1e9, "peak_hbm": hbm, "unit": "GB/s",
+                         "hbm_frac": od_b / (prof_mx["ode_ms"] * 1e-3) / 1e9 / hbm,
+                         "pipes_ncu": PROFILED_ODE_PIPES.get(wl.name)},
         "kernels": {"ode_mixed": {"ms": prof_mx["ode_ms"], "bytes": od_b,
                                   "GBps": od_b / (prof_mx["ode_ms"] * 1e-3) / 1e9},
                     "cg_mixed": {"ms": prof_mx["cg_ms"], "bytes": cg_b,
