@@ -348,6 +348,7 @@ int mb_assemble(const mb_monodomain_desc *d, mb_assembly_out *out) {
         return MB_OK;
     }
     if (d->assembly != MB_ASSEMBLY_ANISOTROPIC) return MB_ERR_ARG;
+    if (d->nx < 1 || d->ny < 1 || d->nz < 1) return MB_ERR_ARG;
 
     /* per-plane tensors; cross terms present? */
     int cross = 0;
