@@ -7,7 +7,9 @@ line with
   - first activation time: max and RMS |difference| in ms over the cells
     activated in both runs, and the number of cells activated in only one;
   - APD90 of the latest beat: max and RMS |difference| in ms over the cells
-    whose beat completed in both runs.
+    whose beat completed in both runs, the number of them above 0.5 ms, and
+    the same over the cells with the same number of activations in both runs
+    (a cell re-excited in one run only measures a different beat).
 
     python -m monoalg3d_c_b200.accuracy_check [--config 1] [--ms 400] [--scale 1.0]
 """
@@ -35,7 +37,8 @@ def _run(wl, precision: str, steps: int):
 def _stats(d: np.ndarray):
     if d.size == 0:
         return {"max": None, "rms": None, "cells": 0}
-    return {"max": float(np.abs(d).max()), "rms": float(np.sqrt(np.mean(d * d))), "cells": int(d.size)}
+    return {"max": float(np.abs(d).max()), "rms": float(np.sqrt(np.mean(d * d))), "cells": int(d.size),
+            "cells_over_0.5": int(np.count_nonzero(np.abs(d) > 0.5))}     # in the block's unit (mV or ms)
 
 
 def main():
@@ -63,6 +66,10 @@ def main():
                               activated_in_one_run_only=int(one.sum())),
         "apd90_ms": _stats(p_mx[apd].astype(np.float64) - p_64[apd].astype(np.float64)),
     }
+    same = apd & (a_mx["count"] == a_64["count"])
+    out["apd90_ms_same_beat_count"] = dict(_stats(p_mx[same].astype(np.float64) - p_64[same].astype(np.float64)),
+                                           activation_count_differs=int(np.count_nonzero(
+                                               a_mx["count"] != a_64["count"])))
     print(json.dumps(out))
 
 
