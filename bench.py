@@ -53,7 +53,9 @@ def parse():
 
 # ---- distributed plumbing (replicas) -----------------------------------------
 
-def dist_init(args):
+def dist_init(args, backend: str = "nccl"):
+    """One process per GPU (RANK / LOCAL_RANK / WORLD_SIZE / MASTER_* from the
+    launcher); the "gloo" backend runs the same plumbing on the CPU."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -61,8 +63,9 @@ def dist_init(args):
         import torch
         import torch.distributed as dist
         import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
 
 
@@ -77,7 +80,7 @@ def allmax(ws, x: float) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
