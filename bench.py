@@ -279,6 +279,9 @@ def model_of(wl):
 
 def main():
     args = parse()
+    # at least 3 untimed warm-up steps, whatever was asked; the line reports
+    # the number taken
+    args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_init(args)
     from monoalg3d_c_b200 import workloads
     wl = workloads.CONFIGS[args.config](args.scale)
