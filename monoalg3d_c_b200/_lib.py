@@ -1,7 +1,8 @@
 """ctypes binding of libmonoalg3d_b200.so (include/monoalg3d_b200.h).
 
-The shared library is built in-tree by ``monoalg3d_c_b200/csrc/Makefile``.
-There is no fallback: if the library is missing, importing this module raises.
+The shared library is built in-tree by ``monoalg3d_c_b200/csrc/Makefile`` and
+loaded at the first call into it.  There is no fallback: if the library is
+missing, that call raises ImportError.
 """
 from __future__ import annotations
 
@@ -184,7 +185,20 @@ def _load() -> C.CDLL:
     return lib
 
 
-lib = _load()
+class _Lazy:
+    """The library, loaded at its first use: importing the package (for
+    the workload descriptions, say) maps no native code; the first call into
+    the library loads it, and raises ImportError if it is missing."""
+
+    _cdll = None
+
+    def __getattr__(self, name):
+        if _Lazy._cdll is None:
+            _Lazy._cdll = _load()
+        return getattr(_Lazy._cdll, name)
+
+
+lib = _Lazy()
 
 
 def check(rc: int) -> None:
