@@ -1,22 +1,31 @@
 """Benchmark of the operator-split monodomain step (cell-steps/s).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config 1] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--repeats R] [--config 4]
+                    [--impl ours|reference]
 
-A step is one iteration of the reference time loop (ODE sub-steps, update_monodomain,
-Jacobi-PCG to r.r <= 1e-16) on the whole tissue.  Default workload: the
-precision configuration, a 200x200x50 slab (2M volumes, 20 % diffuse fibrosis,
-1.6M active) with ToRORd endo cells and fibres along x, run in the
+A step is one iteration of the reference time loop (ODE sub-steps,
+update_monodomain, Jacobi-PCG to r.r <= 1e-16, clock) on the whole tissue.
+Default workload: the scale configuration, a 500x500x100 slab (25 M volumes)
+with ToRORd cells in transmural z-thirds and fibres rotating from +60 to -60
+degrees through the thickness (27-point operator), run in the
 mixed-precision form; the plain FP64 GPU path is timed beside it and the
 mixed/FP64 ratio and the V difference between the two are reported.
 
 value  -- device time of K captured steps (CUDA events on the launching
-          stream), inputs resident in HBM, max over ranks; whole-job cell-steps/s.
+          stream), inputs resident in HBM, max over ranks; the K-step block
+          is timed R times and the median block is reported (all blocks are
+          listed); whole-job cell-steps/s.
 e2e    -- the same steps through the reference-host C-ABI call with host
           buffers: every step copies the stimulus currents host->device and
           V device->host (pinned host buffers).  The headline uses the
           pipelined call (mb_monodomain_step_host_async: the copies of a
           step run under the compute of the next ones, two buffer pairs);
           the synchronous call (mb_monodomain_step_host) is reported beside it.
+--impl reference times the reference's own CPU path (oracle/_ref, OpenMP on
+the host's cores) on the same tissue -- adapter plugins express the
+removed-cell mask, the rotating fibres and the z-layered cell types -- over a
+bounded number of loop steps, by its own clocks; that process maps none of
+this repository's CUDA code.
 Under torchrun each rank runs an independent replica (the path does not shard:
 one GPU solves one tissue), so scaling is weak.
 """
@@ -37,16 +46,20 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 FALLBACK_HBM_GBS = 6650.0
+SMS = 148
+MUFU_PER_SM_CLK = 16          # MUFU (ex2, lg2, rcp, rsqrt) results per SM per clock
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
-    ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 4])
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--repeats", type=int, default=5)
+    ap.add_argument("--config", type=int, default=4, choices=[0, 1, 2, 4])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -88,9 +101,8 @@ def allmax(ws, x: float) -> float:
 # ---- clocks during the timed region ---------------------------------------------
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 100 ms while the
-    timed steps run (the sampler is started just before and stopped just
-    after them)."""
+    """nvidia-smi clocks and throttle reasons sampled every 20 ms while the
+    timed steps run (started just before and stopped just after them)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -100,11 +112,12 @@ class ClockSampler:
         self.gpu = gpu
         self.rows = []
         self.proc = None
+        self.armed = False
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -113,16 +126,21 @@ class ClockSampler:
         return self
 
     def wait_first(self, limit_s: float = 3.0):
+        """Waits for the sampler's first row, then keeps only rows read
+        from here on."""
         t0 = time.time()
+        self.armed = True
         while self.proc and not self.rows and time.time() - t0 < limit_s:
-            time.sleep(0.01)
+            time.sleep(0.005)
         self.rows.clear()
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
+            if self.armed:
+                self.rows.append([c.strip() for c in line.split(",")])
 
     def __exit__(self, *exc):
+        self.armed = False
         if self.proc:
             self.proc.terminate()
             try:
@@ -132,9 +150,9 @@ class ClockSampler:
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[q] for r in self.rows for q in range(4) if len(r) > 5 + q and "Active" in r[5 + q]
                           and "Not" not in r[5 + q]})
@@ -142,43 +160,28 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-# DRAM bytes per launch of the dominant kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum), keyed by workload and CG launch shape:
-#   - from one ncu capture of the same workload and shape
-#     (profiles/k_fcg_group_mixed_slab_200x200x50.md);
-#   - per active cell and CG iteration, from a capture of a smaller case of
-#     the same workload and shape (360x360x72, inputs larger than L2; the
-#     interleaved sweep's traffic grows with the cells), scaled by the
-#     launch's cells and iterations (profiles/k_fcg_group_mixed_slab_500x500x100.md).
-# Keys: (workload, launch shape), else (workload, ("groups", sweep order)) --
-# the four-cell-group shapes of one sweep order read and write the same data,
-# so their DRAM traffic differs only by what L2 keeps between passes.
-PROFILED_TRAFFIC = {("slab_200x200x50_torord_fibrosis20", 10): 145.5e6,
-                    ("slab_200x200x50_torord_fibrosis20", 5): 177.3e6,
-                    ("slab_200x200x50_torord_fibrosis20", ("groups", 0)): 177.3e6}
-PROFILED_TRAFFIC_PER_CELL_ITERATION = {("slab_500x500x100_torord_rotating_fibres", 17): 58.83,
-                                       ("slab_500x500x100_torord_rotating_fibres", ("groups", 1)): 58.83}
-# Pipe utilisation of the mixed ODE kernel from one ncu capture of the same
-# workload (profiles/k_torord_mixed_slab_200x200x50.md): XU = the MUFU pipe
-# (ex2, lg2, rcp, rsqrt: the exp/log/divide-bound part), FMA = the FP32 pipe.
-PROFILED_ODE_PIPES = {"slab_200x200x50_torord_fibrosis20": {"xu_pct": 46.8, "fma_pct": 32.8, "fp64_pct": 1.1,
-                                                            "issue_active_pct": 53.7}}
-FLAT_SHAPES_PER_ORDER = 12     # flat CG shapes per sweep order; the last 7 of each run four-cell groups
+# ---- profiled figures ----------------------------------------------------------------
+#
+# Figures from ncu captures, each keyed by the workload and the exact kernel
+# it was captured on (the CG launch-shape id mb_monodomain_tuning reports, or
+# the ODE kernel's name and variant); a figure is reported only when the
+# bench's tuner picked that same kernel, else the field is null.
+#   (workload, cg kernel id) -> DRAM bytes (dram__bytes_read.sum +
+#   dram__bytes_write.sum) per active cell and CG iteration of one launch
+PROFILED_CG_TRAFFIC = {}
+#   (workload, "mixed" | "fp64", ode variant) -> pipe utilisation and MUFU
+#   (XU pipe) warp instructions x 32 per cell-step of one launch
+PROFILED_ODE = {}
 
 
-def traffic_key(cg_kernel: int):
-    if 0 <= cg_kernel < 2 * FLAT_SHAPES_PER_ORDER and cg_kernel % FLAT_SHAPES_PER_ORDER >= 5:
-        return ("groups", cg_kernel // FLAT_SHAPES_PER_ORDER)
-    return cg_kernel
-
-
-def measured_hbm():
+def measured_peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
         with open(p) as f:
-            return float(json.load(f)["hbm_gbs"]), "measured"
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured", float(d.get("sm_max_mhz", 1965.0))
     except (OSError, KeyError, ValueError):
-        return FALLBACK_HBM_GBS, "fallback"
+        return FALLBACK_HBM_GBS, "fallback", 1965.0
 
 
 # ---- algorithmic bytes (roofline numerators) --------------------------------------
@@ -194,6 +197,13 @@ def cg_bytes(prec: str, n_active: int, n_grid: int, its: float, refinements: flo
     # mixed: x in FP64 (16 B r+w), r and p in FP32 (8 + 8 B); every FP64
     # residual evaluation reads V* and x (16 B) and writes r, p (8 B)
     return n_active * (32.0 * its + 24.0 * max(refinements, 1.0)) + mask
+
+
+def ode_bytes(model: str, prec: str, n_active: int) -> float:
+    """State read + written once per cell-step, plus V in and V* out."""
+    per = {("tt2006", "fp64"): 18 * 8, ("tt2006", "mixed"): 5 * 8 + 13 * 4,
+           ("torord", "fp64"): 42 * 8, ("torord", "mixed"): 8 * 8 + 34 * 4}[(model, prec)]
+    return n_active * (2.0 * per + 16.0)
 
 
 def activation_error(wl, steps: int) -> dict:
@@ -216,43 +226,87 @@ def activation_error(wl, steps: int) -> dict:
             "rms_ms": float(np.sqrt(np.mean(d * d))) if d.size else None}
 
 
-def ode_bytes(model: str, prec: str, n_active: int) -> float:
-    """State read + written once per cell-step, plus V in and V* out."""
-    per = {("tt2006", "fp64"): 18 * 8, ("tt2006", "mixed"): 5 * 8 + 13 * 4,
-           ("torord", "fp64"): 42 * 8, ("torord", "mixed"): 8 * 8 + 34 * 4}[(model, prec)]
-    return n_active * (2.0 * per + 16.0)
-
-
 # ---- arms -------------------------------------------------------------------------
 
-def run_tissue(wl, prec, steps, warmup, ws, gpu):
+def run_tissue(wl, prec, steps, warmup, repeats, ws, gpu):
+    """Creates the tissue, takes `warmup` untimed steps, then times `repeats`
+    blocks of exactly `steps` steps (each bracketed by a barrier and device
+    synchronisation); returns the per-block times (max over ranks)."""
     t = wl.tissue(precision=prec)
     t.step(warmup)
     t.sync()
-    barrier(ws)
+    blocks = []
     with ClockSampler(gpu) as clk:
         clk.wait_first()           # sampler running before the first timed step
-        ms = t.time_steps(steps)
-    t.sync()
-    ms = allmax(ws, ms)
+        for _ in range(repeats):
+            barrier(ws)
+            t.sync()
+            ms = t.time_steps(steps)
+            t.sync()
+            blocks.append(allmax(ws, ms))
     prof = t.profile(3)        # phase times with events: ODE kernel, CG launch
-    stats = t.step_stats(warmup, steps)
-    return t, ms, prof, stats, clk.summary()
+    stats = t.step_stats(warmup, steps * repeats)
+    return t, blocks, prof, stats, clk.summary()
 
 
-def cpu_baseline(wl, model, assembly):
-    """The reference CPU path timed on this host: oracle/_ref (the reference's
-    own build, OpenMP on all physical cores) when it is present, else the C
-    restatement in oracle/ (kind "port", OpenMP)."""
+def reference_case(wl):
     sys.path.insert(0, os.path.join(REPO, "oracle", "ref"))
     import run_reference
-    if not run_reference.available():
+    return run_reference, run_reference.case_from_workload(wl)
+
+
+def host_ram_bytes() -> int:
+    try:
+        import psutil
+        return int(psutil.virtual_memory().available)
+    except ImportError:
+        return 0
+
+
+# host memory the reference's octree grid takes per cell (measured: 1.8 KB
+# per ToRORd cell with the 27-point anisotropic operator on the 25 M-cell
+# slab, 2.3 KB on a 1.6 M-cell one), with a margin
+REF_BYTES_PER_CELL = 2400
+
+
+def reference_sample(rr, case, steps, threads=None, max_cells=None):
+    """The reference CPU path on the case -- or, where the host cannot hold
+    the reference's grid of the whole tissue (or max_cells is smaller), on
+    its first columns at full thickness -- over `steps` loop steps from t = 0;
+    its own clocks."""
+    n = case["nx"] * case["ny"] * case["nz"]
+    ram = host_ram_bytes()
+    budget = ram // REF_BYTES_PER_CELL if ram else n
+    if max_cells:
+        budget = min(budget, max_cells)
+    sub = case
+    if n > budget:
+        f = (budget / n) ** 0.5
+        sx = max(4, int(case["nx"] * f) // 4 * 4)
+        sy = max(4, int(case["ny"] * f) // 4 * 4)
+        sub = rr.sub_block(case, sx, sy)
+    r = rr.time_case(sub, steps, threads=threads)
+    whole = sub is case
+    what = (f"the whole {case['nx']}x{case['ny']}x{case['nz']} tissue" if whole else
+            f"its first {sub['nx']}x{sub['ny']} columns at full thickness ({sub['nx']}x{sub['ny']}x{sub['nz']})")
+    r["sample"] = (f"reference MonoAlg3D CPU path (oracle/_ref: OpenMP, FP64, Jacobi-PCG 1e-16; adapter plugins "
+                   f"for mask / rotating fibres / z-layered cell types) on {what}, {r['steps']} loop steps from "
+                   f"t = 0, Resolution Time - Total Write Time")
+    r["whole_tissue"] = whole
+    return r
+
+
+def cpu_baseline(wl, rr_case):
+    """The reference CPU path timed on this host on a bounded sample of the
+    workload: its first columns at full thickness (at most a million cells),
+    3 loop steps -- 10-30 s of CPU work; the C restatement in oracle/ (kind
+    "port") where the reference build is absent."""
+    rr, case = rr_case
+    if not rr.available():
         return cpu_baseline_port(wl, steps=3)
-    r = run_reference.run(wl.nx, wl.ny, wl.nz, model, assembly, steps=6,
-                          sigma_l=wl.kwargs.get("sigma_l", 0.0002), sigma_t=wl.kwargs.get("sigma_t", 0.00005))
+    r = reference_sample(rr, case, 3, max_cells=1_000_000)
     return {"value": r["cell_steps_per_s"], "unit": "cell-steps/s", "cores": r["threads"], "kind": "reference",
-            "sample": f"reference MonoAlg3D CPU path (OpenMP, FP64, Jacobi-PCG 1e-16) on the {wl.nx}x{wl.ny}x{wl.nz} "
-                      f"cuboid without removed cells, {r['steps']} loop steps, Resolution Time - Write Time"}
+            "sample": r["sample"]}
 
 
 def cpu_baseline_port(wl, steps):
@@ -270,11 +324,35 @@ def cpu_baseline_port(wl, steps):
     threads = int(os.environ.get("OMP_NUM_THREADS", "0")) or (os.cpu_count() or 1)
     return {"value": cells * steps / dt, "unit": "cell-steps/s", "cores": threads, "kind": "port",
             "sample": f"C restatement of the reference CPU path (oracle/, OpenMP, FP64) on the workload "
-                      f"({cells} active cells), {steps} loop steps", "seconds": dt, "steps": steps}
+                      f"({cells} active cells), {steps} loop steps after one untimed step", "seconds": dt,
+            "steps": steps}
 
 
 def model_of(wl):
     return wl.kwargs.get("model", "tt2006")
+
+
+def reference_arm(args, wl, metric):
+    """--impl reference: the reference CPU path on the same workload.  Raises
+    ValueError for inputs no reference plugin expresses."""
+    rr, case = reference_case(wl)
+    if rr.available():
+        r = reference_sample(rr, case, max(args.ref_steps, 3))
+        kind, sample, cells, warm = "reference", r["sample"], r["cells"], 0
+    else:
+        cb = cpu_baseline_port(wl, steps=max(args.ref_steps, 3))
+        r = {"cell_steps_per_s": cb["value"], "seconds": cb["seconds"], "steps": cb["steps"],
+             "threads": cb["cores"], "whole_tissue": True}
+        kind, sample, cells, warm = "port", cb["sample"], wl.active_cells(), 1
+    v = r["cell_steps_per_s"]
+    print(json.dumps({
+        "impl": "reference", "metric": metric, "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
+        "steps": r["steps"], "warmup": warm, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl.name, "cells": wl.n, "active_cells": wl.active_cells(),
+                   "sampled_cells": int(cells), "same_tissue": bool(r["whole_tissue"])},
+        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": r["threads"], "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
 def main():
@@ -282,59 +360,47 @@ def main():
     # at least 3 untimed warm-up steps, whatever was asked; the line reports
     # the number taken
     args.warmup = max(args.warmup, 3)
-    ws, rank, local = dist_init(args)
-    from monoalg3d_c_b200 import workloads
-    wl = workloads.CONFIGS[args.config](args.scale)
-    model = model_of(wl)
-    assembly = wl.kwargs.get("assembly", "homogeneous")
+    args.repeats = max(args.repeats, 1)
     metric = "cell-steps/s (mixed precision)"
+    # the workload descriptions load none of the product's native code
+    from monoalg3d_c_b200 import workloads
     if args.impl == "reference":
-        if rank == 0:
-            sys.path.insert(0, os.path.join(REPO, "oracle", "ref"))
-            import run_reference
-            if not run_reference.available():
-                cb = cpu_baseline_port(wl, steps=max(args.steps // 100, 3))
-                r = {"cell_steps_per_s": cb["value"], "seconds": cb["seconds"], "steps": cb["steps"],
-                     "threads": cb["cores"], "kind": "port", "sample": cb["sample"]}
-            else:
-                r = run_reference.run(wl.nx, wl.ny, wl.nz, model, assembly, steps=max(args.steps // 100, 3),
-                                      sigma_l=wl.kwargs.get("sigma_l", 0.0002),
-                                      sigma_t=wl.kwargs.get("sigma_t", 0.00005))
-            v = r["cell_steps_per_s"]
-            sample = r.get("sample") or (f"reference MonoAlg3D CPU path (OpenMP, FP64) on the {wl.nx}x{wl.ny}x{wl.nz} "
-                                         f"cuboid without removed cells, {r['steps']} loop steps")
-            print(json.dumps({
-                "impl": "reference", "metric": metric, "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
-                "steps": r["steps"], "warmup": 0, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": wl.name, "cells": wl.n},
-                "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": r["threads"],
-                                 "kind": r.get("kind", "reference"), "sample": sample},
-                "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        # rank 0 alone runs the reference; no process group is needed
+        if int(os.environ.get("RANK", "0")) == 0:
+            try:
+                reference_arm(args, workloads.CONFIGS[args.config](args.scale), metric)
+            except ValueError as e:
+                print(json.dumps({"impl": "reference", "unavailable": str(e)}))
         return
+    ws, rank, local = dist_init(args)
+    wl = workloads.CONFIGS[args.config](args.scale)
 
     import ctypes
+    model = model_of(wl)
+    assembly = wl.kwargs.get("assembly", "homogeneous")
     n_active = wl.active_cells()
+    n_grid = wl.n
     masked = wl.kwargs.get("active") is not None
-    t_mx, ms_mx, prof_mx, st_mx, clk_mx = run_tissue(wl, "mixed", args.steps, args.warmup, ws, local)
-    t_64, ms_64, prof_64, st_64, clk_64 = run_tissue(wl, "fp64", args.steps, args.warmup, ws, local)
+    t_mx, bl_mx, prof_mx, st_mx, clk_mx = run_tissue(wl, "mixed", args.steps, args.warmup, args.repeats, ws, local)
+    t_64, bl_64, prof_64, st_64, clk_64 = run_tissue(wl, "fp64", args.steps, args.warmup, args.repeats, ws, local)
+    ms_mx, ms_64 = statistics.median(bl_mx), statistics.median(bl_64)
 
     # V difference of the two forms after the same steps
     v_mx, v_64 = t_mx.v(), t_64.v()
     ok = np.isfinite(v_64)
     dv = v_mx[ok] - v_64[ok]
+    tune_64 = t_64.tuning()
     t_64.close()
 
     # end to end through the reference-host call with pinned host buffers
     import torch
-    n_grid = wl.n
     # The host stimulus of these steps is the merged stimulus the workload's
     # protocol gives at their times.  Untimed steps first move the tissue past
-    # every stimulus window the 2 x steps host-buffer steps would overlap, so
-    # that value is zero -- and it is still copied to the device every step.
+    # every stimulus window the host-buffer steps would overlap, so that value
+    # is zero -- and it is still copied to the device every step.
     dt = wl.kwargs.get("dt_pde", 0.02)
     t0 = t_mx.info()["cur_time"]
-    t_end = t0 + 2 * args.steps * dt
+    t_end = t0 + (args.repeats + 1) * args.steps * dt
     late = [s.start + s.duration for s in wl.kwargs.get("stims", ()) if s.start < t_end and s.start + s.duration > t0]
     if late:
         t_mx.step(int(np.ceil((max(late) - t0) / dt)) + 1)
@@ -347,19 +413,18 @@ def main():
     ms_e2e_sync = t_mx.time_steps_host(args.steps, ctypes.c_void_p(stim.data_ptr()),
                                        ctypes.c_void_p(vout.data_ptr()))
     ms_e2e_sync = allmax(ws, ms_e2e_sync)
-    barrier(ws)
-    ms_e2e = t_mx.time_steps_host_async(args.steps, stim.data_ptr(), stim_b.data_ptr(), vout.data_ptr(),
+    e2e_blocks = []
+    for _ in range(args.repeats):
+        barrier(ws)
+        ms = t_mx.time_steps_host_async(args.steps, stim.data_ptr(), stim_b.data_ptr(), vout.data_ptr(),
                                         vout_b.data_ptr())
-    ms_e2e = allmax(ws, ms_e2e)
+        e2e_blocks.append(allmax(ws, ms))
+    ms_e2e = statistics.median(e2e_blocks)
     tune = t_mx.tuning()
-    t_mx_tuning = tune
     t_mx.close()
-    # activation-time error of the mixed form (untimed, rank 0; 40 ms of the
-    # workload; the 25 M-cell slab is left to the accuracy check module)
-    if rank == 0 and wl.n <= 4_000_000:
-        act_err = activation_error(wl, 2000)
-    else:
-        act_err = {"skipped": "run python -m monoalg3d_c_b200.accuracy_check for this workload"}
+    # activation-time error of the mixed form (untimed, rank 0): 1000 steps
+    # (20 ms) of the workload in both precisions
+    act_err = activation_error(wl, 1000) if rank == 0 else {"skipped": "rank 0 only"}
 
     cell_steps = n_active * args.steps * ws
     value = cell_steps / (ms_mx * 1e-3)
@@ -368,70 +433,78 @@ def main():
     e2e_sync = cell_steps / (ms_e2e_sync * 1e-3)
 
     # roofline of the dominant kernel of the mixed step
-    hbm, hbm_kind = measured_hbm()
+    hbm, hbm_kind, sm_max = measured_peaks()
     its = float(np.mean(st_mx["its"]))
     refs = float(np.mean(st_mx["refinements"]))
     cg_b = cg_bytes("mixed", n_active, n_grid, its, refs, masked)
     od_b = ode_bytes(model, "mixed", n_active)
-    cg_kernel = t_mx_tuning["cg_kernel"]
+    cg_kernel = tune["cg_kernel"]
     if prof_mx["cg_ms"] >= prof_mx["ode_ms"]:
-        form = {100: "k_tcg, 2.5D tiled", 200: "k_rcg, resident tile columns"}.get(cg_kernel, "k_fcg, flat")
-        name, b, dur = f"k_pcg<mixed> ({form} persistent Jacobi-PCG)", cg_b, prof_mx["cg_ms"]
+        name, b, dur = f"persistent Jacobi-PCG<mixed>, launch shape {cg_kernel}", cg_b, prof_mx["cg_ms"]
     else:
         name, b, dur = f"k_{model}_mixed (Rush-Larsen ODE)", od_b, prof_mx["ode_ms"]
     achieved = b / (dur * 1e-3) / 1e9
     traffic, note = None, "algorithmic bytes / CUDA-event time"
-    if name.startswith("k_pcg"):
-        traffic = PROFILED_TRAFFIC.get((wl.name, cg_kernel), PROFILED_TRAFFIC.get((wl.name, traffic_key(cg_kernel))))
-        if traffic is not None:
-            note += "; traffic = DRAM bytes per launch measured by ncu (the solve's working set stays in L2)"
-        per = PROFILED_TRAFFIC_PER_CELL_ITERATION.get(
-            (wl.name, cg_kernel), PROFILED_TRAFFIC_PER_CELL_ITERATION.get((wl.name, traffic_key(cg_kernel))))
-        if per is not None:
-            traffic = per * n_active * its
-            note += ("; traffic = DRAM bytes per cell-iteration measured by ncu on a 360x360x72 case of the "
-                     "same kernel, times the launch's cells and iterations")
+    per = PROFILED_CG_TRAFFIC.get((wl.name, cg_kernel)) if name.startswith("persistent") else None
+    if per is not None:
+        traffic = per * n_active * its
+        note += "; traffic = ncu DRAM bytes per cell-iteration of this kernel, times the launch's cells and iterations"
+    else:
+        note += "; traffic null: no ncu capture of this exact kernel on this workload"
     roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic, "peak_kind": hbm_kind,
             "bytes_per_launch": b, "note": note}
+
+    # ODE roofline: HBM fraction of the state traffic and, where an ncu capture
+    # of the same kernel exists, the MUFU fraction from its instruction census
+    mufu_peak = SMS * MUFU_PER_SM_CLK * sm_max * 1e6
+    ode_roof = {"kernel": f"k_{model}_mixed (Rush-Larsen ODE)", "bound": "sfu/fp32 (MUFU) and hbm",
+                "achieved_hbm": od_b / (prof_mx["ode_ms"] * 1e-3) / 1e9, "peak_hbm": hbm, "unit": "GB/s",
+                "hbm_frac": od_b / (prof_mx["ode_ms"] * 1e-3) / 1e9 / hbm,
+                "mufu_peak_per_s": mufu_peak}
+    for prec, pr, tn in (("mixed", prof_mx, tune), ("fp64", prof_64, tune_64)):
+        p = PROFILED_ODE.get((wl.name, prec, tn["ode_variant"]))
+        cs = n_active / (pr["ode_ms"] * 1e-3)
+        ode_roof[f"{prec}_cell_steps_per_s"] = cs
+        if p:
+            ode_roof[f"ncu_{prec}"] = dict(p, sfu_frac=p["mufu_per_cell_step"] * cs / mufu_peak)
 
     out = {
         "metric": metric, "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_mx / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-        "data": "synthetic (seeded Philox fibrosis mask; workload shapes of the precision configuration)",
+        "data": "synthetic (seeded workload with the configuration's shapes and values)",
         "config": {"workload": wl.name, "cells": n_grid, "active_cells": n_active, "model": model,
                    "assembly": assembly, "dt_ms": 0.02, "cg_tolerance": 1e-16,
                    "l2": "inputs larger than L2 (state + vectors > 126 MB per step)",
-                   "parallelism": f"replicas x{ws}"},
-        "fp64": {"value": fp64_value, "ms_per_step": ms_64 / args.steps,
+                   "parallelism": f"replicas x{ws}", "repeats": args.repeats,
+                   "timed_blocks_ms": bl_mx},
+        "fp64": {"value": fp64_value, "ms_per_step": ms_64 / args.steps, "timed_blocks_ms": bl_64,
                  "cg_iterations_per_step": float(np.mean(st_64["its"])),
-                 "ode_ms": prof_64["ode_ms"], "cg_ms": prof_64["cg_ms"], "clocks": clk_64},
+                 "ode_ms": prof_64["ode_ms"], "cg_ms": prof_64["cg_ms"], "cg_kernel": tune_64["cg_kernel"],
+                 "ode_variant": tune_64["ode_variant"], "clocks": clk_64},
         "mixed_over_fp64": value / fp64_value,
         "mixed": {"ode_ms": prof_mx["ode_ms"], "cg_ms": prof_mx["cg_ms"], "cg_iterations_per_step": its,
                   "fp64_residual_evaluations_per_step": refs, "ode_variant": tune["ode_variant"],
                   "cg_blocks": tune["cg_blocks"], "cg_kernel": tune["cg_kernel"]},
         "error_vs_fp64": {"v_rms_mv": float(np.sqrt(np.mean(dv ** 2))), "v_max_mv": float(np.max(np.abs(dv))),
-                          "after_steps": args.warmup + args.steps + 3, "activation_ms": act_err},
+                          "after_steps": args.warmup + args.steps * args.repeats + 3, "activation_ms": act_err},
         "roofline": roof,
-        "ode_roofline": {"kernel": f"k_{model}_mixed (Rush-Larsen ODE)", "bound": "sfu/fp32 (MUFU) and hbm",
-                         "achieved_hbm": od_b / (prof_mx["ode_ms"] * 1e-3) / 1e9, "peak_hbm": hbm, "unit": "GB/s",
-                         "hbm_frac": od_b / (prof_mx["ode_ms"] * 1e-3) / 1e9 / hbm,
-                         "pipes_ncu": PROFILED_ODE_PIPES.get(wl.name)},
+        "ode_roofline": ode_roof,
         "kernels": {"ode_mixed": {"ms": prof_mx["ode_ms"], "bytes": od_b,
                                   "GBps": od_b / (prof_mx["ode_ms"] * 1e-3) / 1e9},
                     "cg_mixed": {"ms": prof_mx["cg_ms"], "bytes": cg_b,
                                  "GBps": cg_b / (prof_mx["cg_ms"] * 1e-3) / 1e9}},
         "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": n_active * 8,
-                "d2h_bytes_per_step": n_grid * 8,
+                "d2h_bytes_per_step": n_grid * 8, "timed_blocks_ms": e2e_blocks,
                 "call": "mb_monodomain_step_host_async (copies of every step overlapped with the next steps)",
                 "synchronous": {"value": e2e_sync, "call": "mb_monodomain_step_host (copy in, step, copy out, wait)"}},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": 3 * args.steps * args.repeats,
         "clocks": clk_mx,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            out["cpu_baseline"] = cpu_baseline(wl, model, assembly)
+            out["cpu_baseline"] = cpu_baseline(wl, reference_case(wl))
         except Exception as e:  # the baseline is reported, never required
             out["cpu_baseline"] = {"unavailable": str(e)[:200]}
     if rank == 0:
