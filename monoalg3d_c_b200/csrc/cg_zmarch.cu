@@ -1,0 +1,749 @@
+// Persistent Jacobi-PCG for the 27-point operator of fibres rotating through
+// the thickness (kind 2: rows from the per-plane class table), marching
+// through z with every plane of the stencil's input staged in shared memory
+// by the Tensor Memory Accelerator.  Same Krylov recurrences, refinement rule
+// and stopping test as the flat kernel (cg_flat.cu), which follow
+// cpu_conjugate_gradient (src/linear_system_solver_library/linear_system_solver.c:47-183).
+//
+// Why: on the flat kernel each thread gathers the nine rows of a 27-point
+// stencil from L1/L2 with a dependent row -> coefficient -> FMA chain, and the
+// Q pass runs at a quarter of the DRAM rate its bytes allow.  Here a block
+// owns a tile of 128 x W cells (a warp per x-row, four cells per lane) over a
+// range of planes and walks it plane by plane:
+//
+//   TMA   cp.async.bulk.tensor.3d loads the next planes' tiles (with a halo
+//         of 4 cells in x -- the 16-byte alignment of the box -- and 1 in y;
+//         cells outside the grid read as zeros) into S stage buffers, each
+//         completed on its own mbarrier, up to S planes ahead of the compute;
+//   form  each staged plane is turned into the stencil's input in a ring of
+//         four planes: the direction p = r / diag + beta p_old (Q pass; the
+//         Jacobi z is never stored) or x itself (residual pass); the Q pass
+//         stores the new direction's tile cells to global memory here;
+//   apply the output plane k reads planes k-1, k, k+1 of the ring: nine rows
+//         of four cells per lane (one 16-byte shared load each, the values
+//         left and right of the lane's four cells by warp shuffle), summed
+//         in the table's entry order (the same sums as the flat kernel).
+//
+// Each stage buffer and each ring plane is rewritten only after the block
+// barrier that follows its last use, so one __syncthreads per plane orders
+// the pipeline.  Blocks take units (x tile, y tile, z chunk) interleaved, so
+// the blocks of a round work on neighbouring tiles of the same planes and the
+// halo rows they share are read from L2.
+//
+// Per iteration: Q (stencil pass: reads r, p_old; writes p, A p; p.Ap), then
+// U (streaming pass: x += alpha p, r -= alpha A p, r.z and r.r with z = r /
+// diag formed and dropped).  The FP64 residual b - A x (start and
+// refinements) is a stencil pass over x.  Jacobi 1/diag comes from a per-plane
+// table of the nine row classes (1 / the class row's diagonal entry, the value
+// the flat kernel stores per cell).
+//
+// The tensor maps live in global memory (64-byte aligned, written from the
+// host before any launch that reads them).  Every wait is bounded: an
+// mbarrier wait that has not completed after SPIN_LIMIT polls makes the block
+// record MB_ERR_CUDA in the status word, wait (again bounded) for its copies
+// still in flight and leave the kernel; the other blocks then time out at
+// their next grid reduction and leave too.
+#include <cuda.h>
+#include "cg_common.cuh"
+
+namespace mb {
+namespace zcg {
+
+using fcg::Args;
+using fcg::grid_reduce;
+using fcg::SPIN_LIMIT;
+
+constexpr int TX = 128;            // tile width in x: 32 lanes x 4 cells
+constexpr int HX = 4;              // x halo per side (16 bytes of FP32)
+constexpr int WX = TX + 2 * HX;    // staged row length
+constexpr int RING = 4;            // ring planes
+
+struct ZArgs {
+    const double *inv64;           // [nz][9] Jacobi 1/diag per plane and class
+    const float *inv32;
+    // tensor maps of r, p (buffer a), p (buffer b) and x, in global memory
+    const CUtensorMap *maps;
+    int tiles_x, tiles_y, chunks;
+};
+
+__host__ __device__ constexpr int r128(int b) { return (b + 127) / 128 * 128; }
+
+template <typename T, int W, int S>
+struct Lay {
+    static constexpr int H = W + 2;                         // staged rows
+    static constexpr int ELEMS = H * WX;                    // one staged plane
+    static constexpr int ARR = r128(ELEMS * (int)sizeof(T));
+    static constexpr int STAGE = 2 * ARR > r128(ELEMS * 8) ? 2 * ARR : r128(ELEMS * 8);
+    static constexpr int RPLANE = r128(ELEMS * 8);          // ring planes hold doubles (residual pass)
+    static constexpr int BARS = 128;
+    // + 128: the dynamic shared memory base is aligned up to 128 bytes at run
+    // time (bulk tensor copies write to 128-byte-aligned shared addresses)
+    static constexpr int BYTES = BARS + S * STAGE + RING * RPLANE + 128;
+};
+
+// ---- PTX: mbarrier and bulk tensor copies ---------------------------------------
+
+__device__ __forceinline__ uint32_t s32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// The shared-window address of p, computed where the compiler cannot apply
+// what it assumes about p's alignment.
+__device__ __forceinline__ uint32_t smem_addr_opaque(const void *p) {
+    uint32_t a;
+    asm volatile("{\n\t.reg .u64 t;\n\tcvta.to.shared.u64 t, %1;\n\tcvt.u32.u64 %0, t;\n\t}" : "=r"(a) : "l"(p));
+    return a;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *b, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(s32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase with the given parity to complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity) {
+    long long spins = 0;
+    while (!mbar_try_wait(b, parity)) {
+        if (++spins > SPIN_LIMIT) return false;
+        if (spins > 64) __nanosleep(32);
+    }
+    return true;
+}
+// Orders this thread's earlier generic-proxy accesses (and those it has
+// acquired from other threads) before its later async-proxy (TMA) accesses.
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(s32(dst)),
+        "l"(map), "r"(s32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+// ---- vectors of four cells ---------------------------------------------------------
+
+template <typename T>
+struct V4 { T v[4]; };
+
+__device__ __forceinline__ V4<float> ld4(const float *p) {
+    const float4 f = *reinterpret_cast<const float4 *>(p);
+    return {{f.x, f.y, f.z, f.w}};
+}
+__device__ __forceinline__ V4<double> ld4(const double *p) {
+    const double2 a = *reinterpret_cast<const double2 *>(p);
+    const double2 b = *reinterpret_cast<const double2 *>(p + 2);
+    return {{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ void st4(float *p, const V4<float> &v) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v.v[0], v.v[1], v.v[2], v.v[3]);
+}
+__device__ __forceinline__ void st4(double *p, const V4<double> &v) {
+    *reinterpret_cast<double2 *>(p) = make_double2(v.v[0], v.v[1]);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(v.v[2], v.v[3]);
+}
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+template <bool MIXED>
+struct Prec { using T = double; };
+template <>
+struct Prec<true> { using T = float; };
+
+// row class of a cell along one axis: 0 on the low face, 2 on the high face
+__device__ __forceinline__ int axis_class(int i, int n) { return i <= 0 ? 0 : (i >= n - 1 ? 2 : 1); }
+
+template <typename T>
+__device__ __forceinline__ const T *inv_table(const ZArgs &z);
+template <>
+__device__ __forceinline__ const float *inv_table<float>(const ZArgs &z) { return z.inv32; }
+template <>
+__device__ __forceinline__ const double *inv_table<double>(const ZArgs &z) { return z.inv64; }
+
+template <typename T>
+__device__ __forceinline__ T coef(const mb_stencil_dev &st, size_t idx) {
+    if constexpr (sizeof(T) == 8) return __ldg(st.table + idx);
+    else return __ldg(st.table32 + idx);
+}
+
+// ---- units ----------------------------------------------------------------------
+
+struct Unit {
+    int x0, y0, k0, k1;
+};
+
+template <int W>
+__device__ __forceinline__ Unit unit_of(const ZArgs &z, int nz, int u) {
+    const int tx = u % z.tiles_x;
+    const int t = u / z.tiles_x;
+    const int ty = t % z.tiles_y;
+    const int c = t / z.tiles_y;
+    Unit U;
+    U.x0 = tx * TX;
+    U.y0 = ty * W;
+    U.k0 = (int)(((long long)c * nz) / z.chunks);
+    U.k1 = (int)(((long long)(c + 1) * nz) / z.chunks);
+    return U;
+}
+
+// Pipeline state carried across units and passes: the parity each stage's
+// mbarrier completes next.
+struct Pipe {
+    uint32_t phase;
+};
+
+// The 27-point product for the lane's four cells of row j in plane k, from
+// ring planes lo (k-1), mid (k), hi (k+1) (row stride WX, staged row h = the
+// tile row + 1).  Entries of the table row that are zero in every row
+// (st.nzmask) are skipped.  All 32 lanes call it together.
+template <typename R, int W>
+__device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, const R *mid, const R *hi, int k,
+                                         int i0, int j, int w, int lane) {
+    const int cy = axis_class(j, st.ny);
+    int cx[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) cx[c] = axis_class(i0 + c, st.nx);
+    const bool uni = cx[0] == cx[1] && cx[0] == cx[3];
+    size_t row[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) row[c] = ((size_t)k * 9 + (size_t)cy * 3 + (size_t)cx[c]) * 27;
+    R acc[4] = {R(0), R(0), R(0), R(0)};
+    const int off = HX + 4 * lane;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz) {
+        const R *pl = dz < 0 ? lo : (dz == 0 ? mid : hi);
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+            const unsigned rb = (st.nzmask >> ((dz + 1) * 9 + (dy + 1) * 3)) & 7u;
+            if (!rb) continue;
+            const R *rowp = pl + (w + 1 + dy) * WX + off;
+            const V4<R> m4 = ld4(rowp);
+            const R sl = __shfl_up_sync(0xffffffffu, m4.v[3], 1);
+            const R sr = __shfl_down_sync(0xffffffffu, m4.v[0], 1);
+            R wv[6];
+            wv[0] = lane == 0 ? rowp[-1] : sl;
+            wv[5] = lane == 31 ? rowp[4] : sr;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) wv[c + 1] = m4.v[c];
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (!((rb >> (dx + 1)) & 1u)) continue;
+                const int q = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+                const R c0 = coef<R>(st, row[0] + q);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    R cc = c0;
+                    if (c && !uni) cc = coef<R>(st, row[c] + q);
+                    acc[c] = fma(cc, wv[c + 1 + dx], acc[c]);
+                }
+            }
+        }
+    }
+    V4<R> out;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) out.v[c] = acc[c];
+    return out;
+}
+
+// One stencil pass over every unit of this block.  issue(U, m, stage, bar)
+// (thread 0) starts the copies of plane m of unit U into a stage buffer;
+// form(U, m, stage, ring) turns a staged plane into ring plane input;
+// out(U, k, lo, mid, hi) produces output plane k.  Returns false after a wait
+// timed out (the status word is set).
+template <int W, int S, typename IssueF, typename FormF, typename OutF>
+__device__ __forceinline__ bool zpass(const ZArgs &z, const Args &a, unsigned char *smem, int stage_bytes,
+                                      int rplane_bytes, Pipe &pp, IssueF issue, FormF form, OutF out) {
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    unsigned char *stage0 = smem + 128;
+    unsigned char *ring0 = stage0 + (size_t)S * stage_bytes;
+    const int nz = a.st.nz;
+    const int units = z.tiles_x * z.tiles_y * z.chunks;
+    for (int un = blockIdx.x; un < units; un += gridDim.x) {
+        const Unit U = unit_of<W>(z, nz, un);
+        const int P = U.k1 - U.k0 + 2;     // planes k0-1 .. k1
+        if (threadIdx.x == 0) {
+            fence_proxy_async();
+            for (int u = 0; u < S && u < P; ++u) issue(U, U.k0 - 1 + u, stage0 + (size_t)u * stage_bytes, &bars[u]);
+        }
+        for (int u = 0; u < P; ++u) {
+            const int s = u % S;
+            const unsigned par = (pp.phase >> s) & 1u;
+            const bool ok = mbar_wait(&bars[s], par);
+            pp.phase ^= 1u << s;
+            form(U, U.k0 - 1 + u, stage0 + (size_t)s * stage_bytes, ring0 + (size_t)(u & (RING - 1)) * rplane_bytes);
+            if (!__syncthreads_and(ok)) {
+                // copies this block started and has not waited for: plane u
+                // (whose wait gave up) and the ones issued after it
+                if (threadIdx.x == 0) {
+                    atomicExch(a.status, MB_ERR_CUDA);
+                    for (int v = u; v < P && v < u + S; ++v) {
+                        const int sv = v % S;
+                        const unsigned pv = v == u ? par : ((pp.phase >> sv) & 1u);
+                        (void)mbar_wait(&bars[sv], pv);
+                    }
+                }
+                __syncthreads();
+                return false;
+            }
+            if (threadIdx.x == 0 && u + S < P) issue(U, U.k0 - 1 + u + S, stage0 + (size_t)s * stage_bytes, &bars[s]);
+            if (u >= 2) {
+                out(U, U.k0 + u - 2, ring0 + (size_t)((u - 2) & (RING - 1)) * rplane_bytes,
+                    ring0 + (size_t)((u - 1) & (RING - 1)) * rplane_bytes,
+                    ring0 + (size_t)(u & (RING - 1)) * rplane_bytes);
+            }
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
+// ---- the solve ----------------------------------------------------------------
+
+template <bool MIXED, int W, int S, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
+    using T = typename Prec<MIXED>::T;
+    using L = Lay<T, W, S>;
+    // Dynamic shared memory starts after the static reduction arrays of
+    // grid_reduce, at an offset aligned to 16 bytes only; it is declared
+    // with that alignment (a larger declared one would let the compiler
+    // fold the adjustment below away) and aligned up to 128 bytes here, the
+    // address taken through an asm the compiler cannot see through.
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t raw = smem_addr_opaque(smem_raw);
+    unsigned char *smem = smem_raw + ((128u - (raw & 127u)) & 127u);
+    const mb_stencil_dev &st = a.st;
+    mb_ctrl *c = a.ctrl;
+    const bool pre = c->use_precond != 0;
+    const double tol = c->tol;
+    const int max_its = c->max_its;
+    const double ratio = c->refine_ratio;
+    T *__restrict__ r = MIXED ? (T *)a.r32 : (T *)a.r64;
+    T *bufa = MIXED ? (T *)a.pa32 : (T *)a.pa64;
+    T *bufb = MIXED ? (T *)a.pb32 : (T *)a.pb64;
+    T *__restrict__ apb = MIXED ? (T *)a.ap32 : (T *)a.ap64;
+    const T *invt = inv_table<T>(z);
+    const int nx = st.nx, ny = st.ny, nz = st.nz;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    // never issue a copy to a misaligned buffer or through a misaligned map
+    if ((smem_addr_opaque(smem) & 127u) || (reinterpret_cast<uintptr_t>(z.maps) & 63u)) {
+        if (threadIdx.x == 0) atomicExch(a.status, MB_ERR_CUDA);
+        return;
+    }
+    const CUtensorMap *tm_r = z.maps, *tm_pa = z.maps + 1, *tm_pb = z.maps + 2, *tm_x = z.maps + 3;
+    if (threadIdx.x == 0) {
+        // the maps were written by a copy from the host: acquire them for the
+        // tensor-map proxy before the first bulk copy reads them
+        for (int q = 0; q < 4; ++q)
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(z.maps + q) : "memory");
+        for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    Pipe pp{0u};
+    int red = 0;
+
+    // Jacobi 1/diag of a staged or tile cell (i, j) of plane m (clamped into
+    // the grid: values outside it are zero and multiply whatever it returns)
+    auto inv_at = [&](int m, int i, int j) -> T {
+        if (!pre) return T(1);
+        const int mm = m < 0 ? 0 : (m >= nz ? nz - 1 : m);
+        return __ldg(invt + mm * 9 + axis_class(j, ny) * 3 + axis_class(i, nx));
+    };
+
+    // ---- residual pass: r = b - A x (FP64), partials r.z, r.r, r64.r64 ----------
+    auto residual = [&](double (&acc)[3]) -> bool {
+        auto issue = [&](const Unit &U, int m, unsigned char *stg, uint64_t *bar) {
+            mbar_expect_tx(bar, (unsigned)(L::ELEMS * 8));
+            tma_load_3d(stg, tm_x, bar, U.x0 - HX, U.y0 - 1, m);
+        };
+        auto form = [&](const Unit &, int, unsigned char *stg, unsigned char *rp) {
+            const double2 *src = reinterpret_cast<const double2 *>(stg);
+            double2 *dst = reinterpret_cast<double2 *>(rp);
+            for (int e = threadIdx.x; e < L::ELEMS / 2; e += blockDim.x) dst[e] = src[e];
+        };
+        auto out = [&](const Unit &U, int k, unsigned char *lo, unsigned char *mid, unsigned char *hi) {
+            const int j = U.y0 + w, i0 = U.x0 + 4 * lane;
+            if (j >= ny) return;                     // warp-uniform
+            const V4<double> ax = apply27<double, W>(st, reinterpret_cast<const double *>(lo),
+                                                     reinterpret_cast<const double *>(mid),
+                                                     reinterpret_cast<const double *>(hi), k, i0, j, w, lane);
+            if (i0 >= nx) return;
+            const size_t g0 = (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * k);
+            V4<T> rv;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const double bb = a.b ? a.b[g0 + e] : st.alpha * a.vstar[g0 + e];
+                const double r64 = bb - ax.v[e];
+                const T rt = (T)r64;
+                const T zz = pre ? mul_rn(inv_at(k, i0 + e, j), rt) : rt;
+                rv.v[e] = rt;
+                acc[0] += (double)rt * (double)zz;
+                acc[1] += (double)rt * (double)rt;
+                acc[2] += r64 * r64;
+            }
+            st4(r + g0, rv);
+        };
+        return zpass<W, S>(z, a, smem, L::STAGE, L::RPLANE, pp, issue, form, out);
+    };
+
+    // ---- Q pass: p = r / diag + beta p_old, A p, p.Ap ------------------------------
+    auto qpass = [&](bool first, const T *pold, T *pw, double beta, double &q1) -> bool {
+        const CUtensorMap *mp = pold == bufa ? tm_pa : tm_pb;
+        const T bt = (T)beta;
+        auto issue = [&](const Unit &U, int m, unsigned char *stg, uint64_t *bar) {
+            mbar_expect_tx(bar, (unsigned)(L::ELEMS * sizeof(T)) * (first ? 1u : 2u));
+            tma_load_3d(stg, tm_r, bar, U.x0 - HX, U.y0 - 1, m);
+            if (!first) tma_load_3d(stg + L::ARR, mp, bar, U.x0 - HX, U.y0 - 1, m);
+        };
+        auto form = [&](const Unit &U, int m, unsigned char *stg, unsigned char *rp) {
+            const T *rs = reinterpret_cast<const T *>(stg);
+            const T *ps = reinterpret_cast<const T *>(stg + L::ARR);
+            T *dst = reinterpret_cast<T *>(rp);
+            const bool own_plane = m >= U.k0 && m < U.k1;
+            constexpr int QX = WX / 4;
+            for (int e = threadIdx.x; e < L::H * QX; e += blockDim.x) {
+                const int h = e / QX, xq = e - h * QX;
+                const int o = h * WX + 4 * xq;
+                const int i = U.x0 - HX + 4 * xq, j = U.y0 - 1 + h;
+                const V4<T> rv = ld4(rs + o);
+                V4<T> po = {{T(0), T(0), T(0), T(0)}};
+                if (!first) po = ld4(ps + o);
+                // away from the x faces the four cells share one class
+                T iv[4];
+                if (i > 0 && i + 3 < nx - 1) {
+                    iv[0] = iv[1] = iv[2] = iv[3] = inv_at(m, i + 1, j);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) iv[q] = inv_at(m, i + q, j);
+                }
+                V4<T> pv;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const T zz = pre ? mul_rn(iv[q], rv.v[q]) : rv.v[q];
+                    pv.v[q] = first ? zz : fma(bt, po.v[q], zz);
+                }
+                st4(dst + o, pv);
+                if (own_plane && h >= 1 && h <= W && xq >= HX / 4 && xq < (HX + TX) / 4 && i < nx && j < ny)
+                    st4(pw + (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * m), pv);
+            }
+        };
+        auto out = [&](const Unit &U, int k, unsigned char *lo, unsigned char *mid, unsigned char *hi) {
+            const int j = U.y0 + w, i0 = U.x0 + 4 * lane;
+            if (j >= ny) return;
+            const T *pm = reinterpret_cast<const T *>(mid);
+            const V4<T> ap = apply27<T, W>(st, reinterpret_cast<const T *>(lo), pm, reinterpret_cast<const T *>(hi),
+                                           k, i0, j, w, lane);
+            if (i0 >= nx) return;
+            const size_t g0 = (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * k);
+            st4(apb + g0, ap);
+            const V4<T> pc = ld4(pm + (w + 1) * WX + HX + 4 * lane);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) q1 += (double)pc.v[e] * (double)ap.v[e];
+        };
+        return zpass<W, S>(z, a, smem, L::STAGE, L::RPLANE, pp, issue, form, out);
+    };
+
+    // ---- U pass: x += alpha p, r -= alpha A p; r.z, r.r (z formed, not stored) -----
+    auto upass = [&](const T *pc_, double alpha, double (&u2)[2]) {
+        const T al = (T)alpha;
+        double *__restrict__ x = a.x;
+        const unsigned gx = (unsigned)nx >> 2;
+        const unsigned groups = gx * (unsigned)ny * (unsigned)nz;
+        const unsigned step = gridDim.x * blockDim.x;
+        for (unsigned q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < groups; q0 += 2 * step) {
+            V4<T> pv[2], av[2], rv[2];
+            V4<double> xv[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const unsigned q = q0 + u * step;
+                const size_t g0 = (size_t)(q < groups ? q : q0) << 2;
+                pv[u] = ld4(pc_ + g0);
+                av[u] = ld4(apb + g0);
+                rv[u] = ld4(r + g0);
+                xv[u] = ld4(x + g0);
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const unsigned q = q0 + u * step;
+                if (q >= groups) continue;
+                const size_t g0 = (size_t)q << 2;
+                const unsigned t = q / gx;
+                const int i0 = (int)(q - t * gx) << 2;
+                const int k = (int)(t / (unsigned)ny), j = (int)(t - (unsigned)k * (unsigned)ny);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    xv[u].v[e] += alpha * (double)pv[u].v[e];
+                    const T rn = fma(-al, av[u].v[e], rv[u].v[e]);
+                    rv[u].v[e] = rn;
+                    const T zz = pre ? mul_rn(inv_at(k, i0 + e, j), rn) : rn;
+                    u2[0] += (double)zz * (double)rn;
+                    u2[1] += (double)rn * (double)rn;
+                }
+                st4(x + g0, xv[u]);
+                st4(r + g0, rv[u]);
+            }
+        }
+    };
+
+    double acc[3] = {0.0, 0.0, 0.0}, s3[3];
+    if (!residual(acc)) return;
+    if (!grid_reduce<3, 32 * W>(a, acc, s3, red)) return;
+    double rz = s3[0], rr = s3[1];
+    double error = s3[2], rr_ref = s3[2];
+    int its = 1, refinements = MIXED ? 1 : 0;
+    bool done = !(s3[2] >= tol) || !(1 < max_its);
+    bool first = true;
+    double beta = 0.0;
+    T *pcur = bufb;
+
+    while (!done) {
+        T *pnew = pcur == bufa ? bufb : bufa;
+        double q1[1] = {0.0}, s1[1];
+        if (!qpass(first, pcur, pnew, beta, q1[0])) return;
+        if (!grid_reduce<1, 32 * W>(a, q1, s1, red)) return;
+        const double alpha = (pre ? rz : rr) / s1[0];
+        pcur = pnew;
+
+        double u2[2] = {0.0, 0.0}, s2[2];
+        upass(pcur, alpha, u2);
+        if (!grid_reduce<2, 32 * W>(a, u2, s2, red)) return;
+        its += 1;
+        if (!MIXED) {
+            const double b_next = pre ? s2[0] / rz : s2[1] / rr;
+            error = s2[1];
+            if (s2[1] <= tol || its >= max_its) {
+                done = true;
+            } else {
+                beta = b_next;
+                rz = s2[0];
+                rr = s2[1];
+                first = false;
+            }
+        } else {
+            if (s2[1] <= fmax(c->refine_floor, ratio * rr_ref) || its >= max_its) {
+                // FP64 true residual replaces the FP32 recurrence; restart from it
+                double t3[3] = {0.0, 0.0, 0.0};
+                if (!residual(t3)) return;
+                if (!grid_reduce<3, 32 * W>(a, t3, s3, red)) return;
+                refinements += 1;
+                error = s3[2];
+                rr_ref = s3[2];
+                rz = s3[0];
+                rr = s3[1];
+                first = true;
+                if (s3[2] <= tol || its >= max_its) done = true;
+            } else {
+                beta = pre ? s2[0] / rz : s2[1] / rr;
+                rz = s2[0];
+                rr = s2[1];
+                error = s2[1];
+                first = false;
+            }
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c->its = its;
+        c->error = error;
+        c->refinements = refinements;
+        c->rz = rz;
+        c->rr = rr;
+        c->done = 1;
+    }
+}
+
+// Jacobi 1/diag per plane and row class: 1 / the class row's diagonal entry.
+__global__ void k_zinv(mb_stencil_dev st, double *inv64, float *inv32) {
+    const int n = st.nz * 9;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        inv64[e] = 1.0 / st.table[(size_t)e * 27 + 13];
+        inv32[e] = 1.0f / (st.table32 ? st.table32[(size_t)e * 27 + 13] : (float)st.table[(size_t)e * 27 + 13]);
+    }
+}
+
+// ---- variants ---------------------------------------------------------------------
+
+struct Variant {
+    const void *fn;
+    int warps;     // tile rows W (threads = 32 W)
+    int bytes;     // dynamic shared memory
+};
+
+template <bool MIXED, int W, int S, int MINB>
+constexpr Variant make() {
+    return {(const void *)k_zcg<MIXED, W, S, MINB>, W, Lay<typename Prec<MIXED>::T, W, S>::BYTES};
+}
+
+#define MB_ZSHAPES(M) make<M, 8, 3, 1>(), make<M, 8, 3, 2>(), make<M, 16, 3, 1>(), make<M, 4, 3, 3>()
+constexpr int NUM_VARIANTS = 4;
+
+static Variant variant(int mixed, int v) {
+    static const Variant t64[NUM_VARIANTS] = {MB_ZSHAPES(false)};
+    static const Variant t32[NUM_VARIANTS] = {MB_ZSHAPES(true)};
+    return mixed ? t32[v] : t64[v];
+}
+#undef MB_ZSHAPES
+
+// Resident blocks of a variant per SM x SMs (0 where it does not fit).
+static int grid_of(const Variant &var) {
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+    if (cudaFuncSetAttribute(var.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, var.bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, var.fn, 32 * var.warps, var.bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return sms * per;
+}
+
+typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiled encoder() {
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        fn = (EncodeTiled)p;
+    }
+    return fn;
+}
+
+// A 3-D map of an nx x ny x nz grid vector with a box of WX x (W + 2) x 1
+// cells; reads outside the grid return zeros.
+static int encode(CUtensorMap *m, const void *base, int elem, int nx, int ny, int nz, int W) {
+    EncodeTiled fn = encoder();
+    if (!fn || !base) return 0;
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * elem, (cuuint64_t)nx * ny * elem};
+    const cuuint32_t box[3] = {(cuuint32_t)WX, (cuuint32_t)(W + 2), 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = fn(m, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                          const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+}  // namespace zcg
+}  // namespace mb
+
+using namespace mb::zcg;
+
+extern "C" int mbk_zcg_variants(void) { return NUM_VARIANTS; }
+
+// Grid size of variant v (blocks resident at once), 0 if it cannot run.
+extern "C" int mbk_zcg_max_blocks(int mixed, int v) {
+    if (v < 0 || v >= NUM_VARIANTS) return 0;
+    return grid_of(variant(mixed, v));
+}
+
+// Whether the z-march kernel applies: the 27-point class-table operator on a
+// grid whose rows are whole 16-byte vectors (nx % 4 == 0).
+extern "C" int mbk_zcg_usable(const mb_stencil_dev *st) {
+    return st->kind == 2 && st->nx % 4 == 0 && st->nx >= 4 && st->ny >= 1 && st->nz >= 1 && st->table &&
+           st->table32;
+}
+
+// Per-plane Jacobi tables (device arrays of nz * 9 values each).
+extern "C" int mbk_zcg_inv_tables(const mb_stencil_dev *st, double *inv64, float *inv32, cudaStream_t s) {
+    k_zinv<<<(st->nz * 9 + 255) / 256, 256, 0, s>>>(*st, inv64, inv32);
+    return (int)cudaGetLastError();
+}
+
+// Tensor maps of every variant (4 per variant: r, p buffer a, p buffer b,
+// x), encoded on the host and copied to a device array p->zc_maps allocated
+// here (freed by the tissue).  Called once the CG buffers exist, before any
+// launch or stream capture.  Returns 0 or a CUDA error code.
+extern "C" int mbk_zcg_prepare(mb_pcg_dev *p) {
+    const int nx = p->st.nx, ny = p->st.ny, nz = p->st.nz;
+    const int elem = p->mixed ? 4 : 8;
+    alignas(64) CUtensorMap tm[NUM_VARIANTS * 4];
+    const void *bases[4] = {p->mixed ? (const void *)p->r32 : (const void *)p->r64,
+                            p->mixed ? (const void *)p->pa32 : (const void *)p->pa64,
+                            p->mixed ? (const void *)p->pb32 : (const void *)p->pb64, (const void *)p->x};
+    for (int v = 0; v < NUM_VARIANTS; ++v)
+        for (int q = 0; q < 4; ++q)
+            if (!encode(&tm[4 * v + q], bases[q], q == 3 ? 8 : elem, nx, ny, nz, variant(p->mixed, v).warps))
+                return (int)cudaErrorInvalidValue;
+    if (!p->zc_maps) {
+        cudaError_t e = cudaMalloc(&p->zc_maps, sizeof tm);
+        if (e != cudaSuccess) return (int)e;
+    }
+    return (int)cudaMemcpy(p->zc_maps, tm, sizeof tm, cudaMemcpyHostToDevice);
+}
+
+extern "C" int mbk_zcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
+    if (p->zc_variant < 0 || p->zc_variant >= NUM_VARIANTS || !p->zc_maps) return (int)cudaErrorInvalidValue;
+    const Variant var = variant(p->mixed, p->zc_variant);
+    const int nx = p->st.nx, ny = p->st.ny, nz = p->st.nz;
+    const int blocks = p->blocks;
+    if (blocks <= 0) return (int)cudaErrorInvalidConfiguration;
+    // units: x tiles of 128 cells, y tiles of W rows, z chunks; the number of
+    // chunks minimises the rounds of units the grid takes times the planes a
+    // unit walks (its planes plus the two halo planes)
+    ZArgs z;
+    z.inv64 = p->zc_inv64;
+    z.inv32 = p->zc_inv32;
+    z.maps = reinterpret_cast<const CUtensorMap *>(p->zc_maps) + 4 * p->zc_variant;
+    z.tiles_x = (nx + TX - 1) / TX;
+    z.tiles_y = (ny + var.warps - 1) / var.warps;
+    {
+        long long best = -1;
+        int bc = 1;
+        for (int c = 1; c <= nz && c <= 64; ++c) {
+            const long long units = (long long)z.tiles_x * z.tiles_y * c;
+            const long long rounds = (units + blocks - 1) / blocks;
+            const long long cost = rounds * ((nz + c - 1) / c + 2);
+            if (best < 0 || cost < best) {
+                best = cost;
+                bc = c;
+            }
+        }
+        z.chunks = bc;
+    }
+    Args a;
+    a.st = p->st;
+    a.x = p->x; a.vstar = p->vstar; a.b = p->b;
+    a.r64 = p->r64; a.pa64 = p->pa64; a.pb64 = p->pb64; a.z64 = p->z64;
+    a.r32 = p->r32; a.pa32 = p->pa32; a.pb32 = p->pb32; a.z32 = p->z32;
+    a.ap64 = p->ap64; a.ap32 = p->ap32;
+    a.inv_diag64 = p->inv_diag64; a.inv_diag32 = p->inv_diag32;
+    a.partials = p->partials; a.ctrl = p->ctrl; a.bar = p->bar; a.status = p->status;
+    cudaError_t e = cudaMemsetAsync(p->bar, 0, 2 * sizeof(unsigned), s);
+    if (e != cudaSuccess) return (int)e;
+    void *args[] = {&a, &z};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(32 * var.warps);
+    cfg.dynamicSmemBytes = var.bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return (int)cudaLaunchKernelExC(&cfg, var.fn, args);
+}

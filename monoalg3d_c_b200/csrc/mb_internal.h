@@ -193,8 +193,14 @@ typedef struct mb_pcg_dev {
     int rc_shape, rc_nbx, rc_nby, rc_tw, rc_th;
     size_t rc_smem;
     double *rtrue;           /* resident kernel: FP64 true residual per cell */
+    /* z-march kernel (cg_zmarch.cu): variant, per-plane Jacobi tables
+     * (nz x 9 row classes) and the device array of its tensor maps */
+    int zc_variant;
+    double *zc_inv64;
+    float *zc_inv32;
+    void *zc_maps;
 } mb_pcg_dev;
-enum { MB_PCG_FLAT = 0, MB_PCG_TILED = 1, MB_PCG_RESIDENT = 2 };
+enum { MB_PCG_FLAT = 0, MB_PCG_TILED = 1, MB_PCG_RESIDENT = 2, MB_PCG_ZMARCH = 3 };
 int mbk_fcg_variants(int kind);
 int mbk_fcg_variant_groups(int variant);
 int mbk_fcg_max_blocks(int mixed, int kind, int variant);
@@ -205,6 +211,12 @@ void mbk_tcg_layout(int nx, int ny, int nz, int blocks, int *tiles_x, int *tiles
 int mbk_rcg_plan(mb_pcg_dev *p);
 int mbk_rcg_launch(const mb_pcg_dev *p, cudaStream_t s);
 int mbk_inv_diag(const mb_stencil_dev *st, double *d64, float *d32, cudaStream_t s);
+int mbk_zcg_variants(void);
+int mbk_zcg_max_blocks(int mixed, int variant);
+int mbk_zcg_usable(const mb_stencil_dev *st);
+int mbk_zcg_inv_tables(const mb_stencil_dev *st, double *inv64, float *inv32, cudaStream_t s);
+int mbk_zcg_prepare(mb_pcg_dev *p);
+int mbk_zcg_launch(const mb_pcg_dev *p, cudaStream_t s);
 
 /* Pseudo-bidomain ECG at the start of a step (ecg.cu). */
 typedef struct mb_ecg_dev {

@@ -305,7 +305,7 @@ void mb_monodomain_destroy(mb_monodomain *m) {
                     m->d_partials, m->d_sv64, m->d_sv32, m->d_stim_bits, m->d_celltype, m->d_scale,
                     m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_code, m->d_rowid, m->d_act,
                     m->d_stim_host, m->d_ctrl, m->d_log, m->d_stim2[0], m->d_stim2[1], m->d_vsnap[0],
-                    m->d_vsnap[1]};
+                    m->d_vsnap[1], m->pcg.zc_inv64, m->pcg.zc_inv32, m->pcg.zc_maps};
     for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
     for (int i = 0; i < 4; ++i) if (m->ev[i]) cudaEventDestroy(m->ev[i]);
     for (int i = 0; i < 4; ++i)
@@ -374,16 +374,19 @@ static int pcg_launch(const mb_pcg_dev *q, cudaStream_t s) {
     switch (q->form) {
     case MB_PCG_TILED: return mbk_tcg_launch(q, s);
     case MB_PCG_RESIDENT: return mbk_rcg_launch(q, s);
+    case MB_PCG_ZMARCH: return mbk_zcg_launch(q, s);
     default: return mbk_fcg_launch(q, s);
     }
 }
 
 /* Picks the CG kernel: every launch-shape variant of the flat persistent
- * kernel, the 2.5D tiled one and, where its tiles fit, the resident one solve
- * the tissue's first system (b = alpha V* from the initial state) twice; V is
- * restored after every trial and the fastest by CUDA events is kept.
- * MB_CG_VARIANT=<n> forces a choice (n = number of flat variants selects the
- * tiled kernel, one more the resident kernel). */
+ * kernel, the 2.5D tiled one, where its tiles fit the resident one and, for
+ * the 27-point class-table operator, every variant of the z-march kernel
+ * solve the tissue's first system (b = alpha V* from the initial state)
+ * twice; V is restored after every trial and the fastest by CUDA events is
+ * kept.  MB_CG_VARIANT=<n> forces a choice (n = number of flat variants
+ * selects the tiled kernel, n + 1 the resident kernel, n + 2 + v z-march
+ * variant v). */
 static int cg_autotune(mb_monodomain *m) {
     if (!m->use_pcg) return MB_OK;
     const int mixed = m->pcg.mixed;
@@ -398,8 +401,11 @@ static int cg_autotune(mb_monodomain *m) {
         }
         m->pcg.rtrue = m->d_rtrue;
     }
+    const int zmarch = mbk_zcg_usable(&m->st) && m->pcg.zc_maps != NULL;
+    const int nzv = mbk_zcg_variants();
     const char *env = getenv("MB_CG_VARIANT");
-    int lo = 0, hi = nv + 1;      /* candidates 0..nv-1 flat, nv tiled, nv+1 resident */
+    /* candidates 0..nv-1 flat, nv tiled, nv+1 resident, nv+2.. z-march */
+    int lo = 0, hi = nv + 1 + (zmarch ? nzv : 0);
     if (env) lo = hi = atoi(env);
     double *vsave = NULL;
     if (cudaMalloc((void **)&vsave, (size_t)m->n * sizeof(double)) != cudaSuccess)
@@ -418,10 +424,15 @@ static int cg_autotune(mb_monodomain *m) {
             const int items = q.tiles_x * q.tiles_y * q.nchunks;
             const int mb = mbk_tcg_max_blocks(mixed);
             q.blocks = items < mb ? items : mb;
-        } else {
+        } else if (cand == nv + 1) {
             if (!resident) continue;
             q.form = MB_PCG_RESIDENT;
             q.blocks = q.rc_nbx * q.rc_nby;
+        } else {
+            if (!zmarch || cand - nv - 2 >= nzv) continue;
+            q.form = MB_PCG_ZMARCH;
+            q.zc_variant = cand - nv - 2;
+            q.blocks = mbk_zcg_max_blocks(mixed, q.zc_variant);
         }
         if (q.blocks <= 0) continue;
         if (cand < nv && mbk_fcg_variant_groups(cand) && (m->desc.nx % 4) != 0) continue;
@@ -461,9 +472,13 @@ static int cg_autotune(mb_monodomain *m) {
         const int items = m->pcg.tiles_x * m->pcg.tiles_y * m->pcg.nchunks;
         const int mb = mbk_tcg_max_blocks(mixed);
         m->pcg.blocks = items < mb ? items : mb;
-    } else {
+    } else if (bestc == nv + 1) {
         m->pcg.form = MB_PCG_RESIDENT;
         m->pcg.blocks = m->pcg.rc_nbx * m->pcg.rc_nby;
+    } else {
+        m->pcg.form = MB_PCG_ZMARCH;
+        m->pcg.zc_variant = bestc - nv - 2;
+        m->pcg.blocks = mbk_zcg_max_blocks(mixed, m->pcg.zc_variant);
     }
     if (m->pcg.form != MB_PCG_RESIDENT && m->d_rtrue) {
         cudaFree(m->d_rtrue);
@@ -709,6 +724,11 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
             }
             const int bt = mbk_tcg_max_blocks(mixed);
             if (bt > maxb) maxb = bt;
+            if (mbk_zcg_usable(&m->st))
+                for (int v = 0; v < mbk_zcg_variants(); ++v) {
+                    const int b = mbk_zcg_max_blocks(mixed, v);
+                    if (b > maxb) maxb = b;
+                }
             mbk_tcg_layout(d->nx, d->ny, d->nz, bt > 0 ? bt : 1, &m->pcg.tiles_x, &m->pcg.tiles_y, &m->pcg.zchunk,
                            &m->pcg.nchunks);
         }
@@ -739,6 +759,11 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
                 CKK(cudaMemset(m->d_invd32, 0, (size_t)n * sizeof(float)));
             }
             CKK(mbk_inv_diag(&m->st, m->d_invd, m->d_invd32, m->stream));
+            if (mbk_zcg_usable(&m->st)) {
+                ALLOC(m->pcg.zc_inv64, (size_t)d->nz * 9 * sizeof(double));
+                ALLOC(m->pcg.zc_inv32, (size_t)d->nz * 9 * sizeof(float));
+                CKK(mbk_zcg_inv_tables(&m->st, m->pcg.zc_inv64, m->pcg.zc_inv32, m->stream));
+            }
             CKK(cudaStreamSynchronize(m->stream));
             ALLOC(m->d_bar, 2 * sizeof(unsigned));
             ALLOC(m->d_status, sizeof(int));
@@ -763,6 +788,8 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
             q->inv_diag32 = m->d_invd32;
             q->bar = m->d_bar;
             q->status = m->d_status;
+            q->st = m->st;
+            if (q->zc_inv64) CKK(mbk_zcg_prepare(q));
         }
     }
 
@@ -939,7 +966,8 @@ int mb_monodomain_tuning(mb_monodomain *m, int *ode_variant, int *cg_blocks, int
     if (cg_kernel)
         *cg_kernel = !m->use_pcg ? -1
                    : m->pcg.form == MB_PCG_TILED ? 100
-                   : m->pcg.form == MB_PCG_RESIDENT ? 200 : m->pcg.variant;
+                   : m->pcg.form == MB_PCG_RESIDENT ? 200
+                   : m->pcg.form == MB_PCG_ZMARCH ? 300 + m->pcg.zc_variant : m->pcg.variant;
     return MB_OK;
 }
 

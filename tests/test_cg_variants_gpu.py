@@ -1,6 +1,7 @@
 """Every launch shape of the persistent CG (one cell per thread, U cells per
 thread, four-cell groups, each with per-block ranges and interleaved sweeps;
-2.5D tiles) against the CPU oracle on each
+2.5D tiles; for the 27-point operator the z-march kernel's variants, whose
+stencil input is staged by TMA) against the CPU oracle on each
 operator kind: constant coefficients with removed cells, per-cell
 conductivity, and the 27-point rows of fibres rotating through the wall.
 The shape the autotuner would pick is forced through MB_CG_VARIANT, which
@@ -21,6 +22,14 @@ import oracle  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 STEPS = 120
+ZMARCH_VARIANTS = 4
+
+
+def _kernel_id(v: int, nf: int) -> int:
+    """The cg_kernel id mb_monodomain_tuning reports for MB_CG_VARIANT=v."""
+    if v < nf:
+        return v
+    return {nf: 100, nf + 1: 200}.get(v, 300 + (v - nf - 2))
 
 
 def _cases():
@@ -48,14 +57,17 @@ def test_every_launch_shape_matches_oracle(case):
     o.close()
     ok = np.isfinite(ref)
     from monoalg3d_c_b200.monodomain import cg_launch_shapes
-    nv = cg_launch_shapes() + 1                  # flat shapes (two sweep orders) + the tiled kernel
+    nf = cg_launch_shapes()
+    # flat shapes (two sweep orders), the tiled kernel, and for the 27-point
+    # operator the z-march variants (MB_CG_VARIANT nf + 2 + v)
+    variants = list(range(nf + 1)) + ([nf + 2 + z for z in range(ZMARCH_VARIANTS)] if case == "rotating" else [])
     old = os.environ.get("MB_CG_VARIANT")
     try:
-        for v in range(nv):
+        for v in variants:
             os.environ["MB_CG_VARIANT"] = str(v)
             t = Tissue(nx, ny, nz, precision="fp64", stims=stims, **kw)
             kernel = t.tuning()["cg_kernel"]
-            assert kernel == (100 if v == nv - 1 else v), f"variant {v} not used ({kernel})"
+            assert kernel == _kernel_id(v, nf), f"variant {v} not used ({kernel})"
             t.step(STEPS)
             got = t.v()
             t.close()
@@ -83,14 +95,15 @@ def test_every_launch_shape_mixed(case):
     old = os.environ.get("MB_CG_VARIANT")
     its0 = None
     try:
-        for v in range(nf + 2):                   # flat shapes, tiled, resident
+        variants = list(range(nf + 2)) + ([nf + 2 + z for z in range(ZMARCH_VARIANTS)] if case == "rotating" else [])
+        for v in variants:                        # flat shapes, tiled, resident, z-march
             os.environ["MB_CG_VARIANT"] = str(v)
             t = Tissue(nx, ny, nz, precision="mixed", stims=stims, **kw)
             kernel = t.tuning()["cg_kernel"]
             if v == nf + 1 and kernel != 200:
                 t.close()                         # the resident kernel does not apply to this operator
                 continue
-            assert kernel == {nf: 100, nf + 1: 200}.get(v, v), f"variant {v} not used ({kernel})"
+            assert kernel == _kernel_id(v, nf), f"variant {v} not used ({kernel})"
             t.step(STEPS)
             got = t.v()
             its = t.step_stats(0, STEPS)["its"]

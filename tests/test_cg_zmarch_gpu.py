@@ -1,0 +1,89 @@
+"""The z-march CG (cg_zmarch.cu: TMA-staged planes, tiles of 128 x W cells over
+z chunks) on grids that exercise its tiling: several x tiles with a partial
+last one, partial y tiles, several z chunks, and the rows' x / y face
+classes at tile edges.  Every variant (forced through MB_CG_VARIANT) against
+the CPU oracle after 60 steps of the rotating-fibre operator, ToRORd with
+z-layered cell types: FP64 within 1e-8 relative with the oracle's CG
+iteration count at every step; mixed precision within 2e-3 relative (+1 mV)
+with iteration counts within one of the flat kernel's."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import oracle  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 60
+ZMARCH_VARIANTS = 4
+
+
+def _case():
+    from monoalg3d_c_b200 import workloads
+    nx, ny, nz = 264, 21, 7          # x tiles 128 + 128 + 8, y tiles partial for every W
+    kw = dict(model="torord", assembly="anisotropic", sigma_l=0.0002, sigma_t=0.00004, sigma_n=0.00004,
+              fibre_angle_z=workloads.fibre_angles(nz), celltype=workloads.transmural_thirds(nx, ny, nz),
+              stims=[workloads.planar_stim()])
+    return nx, ny, nz, kw
+
+
+def _run(precision, v, nx, ny, nz, kw):
+    from monoalg3d_c_b200 import Tissue
+    old = os.environ.get("MB_CG_VARIANT")
+    try:
+        os.environ["MB_CG_VARIANT"] = str(v)
+        t = Tissue(nx, ny, nz, precision=precision, **kw)
+    finally:
+        if old is None:
+            os.environ.pop("MB_CG_VARIANT", None)
+        else:
+            os.environ["MB_CG_VARIANT"] = old
+    kernel = t.tuning()["cg_kernel"]
+    t.step(STEPS)
+    v_out = t.v()
+    its = t.step_stats(0, STEPS)["its"]
+    t.close()
+    return kernel, v_out, its
+
+
+@pytest.fixture(scope="module")
+def reference():
+    nx, ny, nz, kw = _case()
+    o = oracle.Sim(nx, ny, nz, **kw)
+    its = []
+    for _ in range(STEPS):
+        o.step(1)
+        its.append(o.last_cg()[0])
+    ref = o.v()
+    o.close()
+    return ref, np.array(its)
+
+
+@pytest.mark.parametrize("z", range(ZMARCH_VARIANTS))
+def test_zmarch_fp64_matches_oracle(reference, z):
+    from monoalg3d_c_b200.monodomain import cg_launch_shapes
+    ref, its_ref = reference
+    nx, ny, nz, kw = _case()
+    nf = cg_launch_shapes()
+    kernel, got, its = _run("fp64", nf + 2 + z, nx, ny, nz, kw)
+    assert kernel == 300 + z
+    err = np.abs(got - ref)
+    assert np.all(err <= 1e-8 * np.abs(ref) + 1e-9), f"variant {z}: max |dV| {err.max():.3e}"
+    assert np.array_equal(its, its_ref), f"variant {z}: CG iterations {its} vs oracle {its_ref}"
+
+
+@pytest.mark.parametrize("z", range(ZMARCH_VARIANTS))
+def test_zmarch_mixed_matches_oracle_and_flat(reference, z):
+    from monoalg3d_c_b200.monodomain import cg_launch_shapes
+    ref, _ = reference
+    nx, ny, nz, kw = _case()
+    nf = cg_launch_shapes()
+    _, _, its_flat = _run("mixed", 0, nx, ny, nz, kw)
+    kernel, got, its = _run("mixed", nf + 2 + z, nx, ny, nz, kw)
+    assert kernel == 300 + z
+    err = np.abs(got - ref)
+    assert np.all(err <= 2e-3 * (np.abs(ref) + 1.0)), f"variant {z}: max |dV| {err.max():.3e}"
+    assert np.abs(its - its_flat).max() <= 1
