@@ -58,15 +58,32 @@ constexpr int HX = 4;              // x halo per side (16 bytes of FP32)
 constexpr int WX = TX + 2 * HX;    // staged row length
 constexpr int RING = 4;            // ring planes
 
+// Division by a fixed divisor d as a multiply and shifts (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", 1994,
+// round-up form): with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (t + ((n - t) >> 1)) >> (l - 1) for t = mulhi(m, n), every 32-bit n.
+struct FastDiv {
+    uint32_t d, m, l;
+    __device__ __forceinline__ uint32_t div(uint32_t n) const {
+        if (d == 1) return n;
+        const uint32_t t = __umulhi(m, n);
+        return (t + ((n - t) >> 1)) >> (l - 1);
+    }
+};
+
 struct ZArgs {
     const double *inv64;           // [nz][9] Jacobi 1/diag per plane and class
     const float *inv32;
     // tensor maps of r, p (buffer a), p (buffer b) and x, in global memory
     const CUtensorMap *maps;
     int tiles_x, tiles_y, chunks;
+    FastDiv by_gx, by_ny;          // n / (nx / 4), n / ny
 };
 
 __host__ __device__ constexpr int r128(int b) { return (b + 127) / 128 * 128; }
+
+constexpr int TSLOTS = 4;          // per-plane table slots
+constexpr int TROW = 9 * 27 + 9;   // one plane: 9 class rows of 27 entries, 9 Jacobi values
 
 template <typename T, int W, int S>
 struct Lay {
@@ -76,9 +93,12 @@ struct Lay {
     static constexpr int STAGE = 2 * ARR > r128(ELEMS * 8) ? 2 * ARR : r128(ELEMS * 8);
     static constexpr int RPLANE = r128(ELEMS * 8);          // ring planes hold doubles (residual pass)
     static constexpr int BARS = 128;
+    // the coefficient rows and Jacobi values of up to four planes, both
+    // precisions (the residual pass applies the FP64 rows)
+    static constexpr int TABS = r128(TSLOTS * TROW * 8) + r128(TSLOTS * TROW * 4);
     // + 128: the dynamic shared memory base is aligned up to 128 bytes at run
     // time (bulk tensor copies write to 128-byte-aligned shared addresses)
-    static constexpr int BYTES = BARS + S * STAGE + RING * RPLANE + 128;
+    static constexpr int BYTES = BARS + TABS + S * STAGE + RING * RPLANE + 128;
 };
 
 // ---- PTX: mbarrier and bulk tensor copies ---------------------------------------
@@ -203,21 +223,19 @@ struct Pipe {
     uint32_t phase;
 };
 
-// The 27-point product for the lane's four cells of row j in plane k, from
-// ring planes lo (k-1), mid (k), hi (k+1) (row stride WX, staged row h = the
-// tile row + 1).  Entries of the table row that are zero in every row
-// (st.nzmask) are skipped.  All 32 lanes call it together.
+// The 27-point product for the lane's four cells of row j, from ring planes
+// lo (k-1), mid (k), hi (k+1) (row stride WX, staged row h = the tile row +
+// 1) and the plane's class rows ct (9 rows of 27 entries in shared memory).
+// Every cell is first summed with the row of its y class and the interior x
+// class (the same row for the whole warp); lanes holding a cell on an x face
+// (i = 0 or nx - 1) then redo that cell with its own row.  Entries that are
+// zero in every row (st.nzmask) are skipped; sums run in entry order.  All 32
+// lanes call it together.
 template <typename R, int W>
-__device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, const R *mid, const R *hi, int k,
-                                         int i0, int j, int w, int lane) {
+__device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, const R *mid, const R *hi,
+                                         const R *ct, int i0, int j, int w, int lane) {
     const int cy = axis_class(j, st.ny);
-    int cx[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) cx[c] = axis_class(i0 + c, st.nx);
-    const bool uni = cx[0] == cx[1] && cx[0] == cx[3];
-    size_t row[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) row[c] = ((size_t)k * 9 + (size_t)cy * 3 + (size_t)cx[c]) * 27;
+    const R *cm = ct + (cy * 3 + 1) * 27;
     R acc[4] = {R(0), R(0), R(0), R(0)};
     const int off = HX + 4 * lane;
 #pragma unroll
@@ -240,15 +258,29 @@ __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, 
             for (int dx = -1; dx <= 1; ++dx) {
                 if (!((rb >> (dx + 1)) & 1u)) continue;
                 const int q = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-                const R c0 = coef<R>(st, row[0] + q);
+                const R cc = cm[q];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    R cc = c0;
-                    if (c && !uni) cc = coef<R>(st, row[c] + q);
-                    acc[c] = fma(cc, wv[c + 1 + dx], acc[c]);
+                for (int c = 0; c < 4; ++c) acc[c] = fma(cc, wv[c + 1 + dx], acc[c]);
+            }
+        }
+    }
+    // cells on an x face: only the lanes holding one take this branch
+    const int e = i0 == 0 ? 0 : (i0 + 3 == st.nx - 1 ? 3 : -1);
+    if (e >= 0) {
+        const R *ce = ct + (cy * 3 + axis_class(i0 + e, st.nx)) * 27;
+        R a = R(0);
+        for (int dz = -1; dz <= 1; ++dz) {
+            const R *pl = dz < 0 ? lo : (dz == 0 ? mid : hi);
+            for (int dy = -1; dy <= 1; ++dy) {
+                const R *rowp = pl + (w + 1 + dy) * WX + off + e;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int q = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+                    if ((st.nzmask >> q) & 1u) a = fma(ce[q], rowp[dx], a);
                 }
             }
         }
+        if (e == 0) acc[0] = a;
+        else acc[3] = a;
     }
     V4<R> out;
 #pragma unroll
@@ -261,11 +293,18 @@ __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, 
 // form(U, m, stage, ring) turns a staged plane into ring plane input;
 // out(U, k, lo, mid, hi) produces output plane k.  Returns false after a wait
 // timed out (the status word is set).
-template <int W, int S, typename IssueF, typename FormF, typename OutF>
-__device__ __forceinline__ bool zpass(const ZArgs &z, const Args &a, unsigned char *smem, int stage_bytes,
-                                      int rplane_bytes, Pipe &pp, IssueF issue, FormF form, OutF out) {
+//
+// Plane v of a unit (plane k0 - 1 + v) has its coefficient rows and Jacobi
+// values in table slot v % 4: loaded (tabs(m, slot)) in step v - 1 (the
+// prologue for v = 0) before that step's barrier, read by the form of step v
+// and the output of step v + 1, and rewritten in step v + 3 -- after the
+// barrier of step v + 2, which every reader of step v + 1 has passed.
+template <int W, int S, typename IssueF, typename TabF, typename FormF, typename OutF>
+__device__ __forceinline__ bool zpass(const ZArgs &z, const Args &a, unsigned char *smem, int tabs_bytes,
+                                      int stage_bytes, int rplane_bytes, Pipe &pp, IssueF issue, TabF tabs,
+                                      FormF form, OutF out) {
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-    unsigned char *stage0 = smem + 128;
+    unsigned char *stage0 = smem + 128 + tabs_bytes;
     unsigned char *ring0 = stage0 + (size_t)S * stage_bytes;
     const int nz = a.st.nz;
     const int units = z.tiles_x * z.tiles_y * z.chunks;
@@ -276,12 +315,16 @@ __device__ __forceinline__ bool zpass(const ZArgs &z, const Args &a, unsigned ch
             fence_proxy_async();
             for (int u = 0; u < S && u < P; ++u) issue(U, U.k0 - 1 + u, stage0 + (size_t)u * stage_bytes, &bars[u]);
         }
+        tabs(U.k0 - 1, 0);
+        __syncthreads();
         for (int u = 0; u < P; ++u) {
             const int s = u % S;
             const unsigned par = (pp.phase >> s) & 1u;
             const bool ok = mbar_wait(&bars[s], par);
             pp.phase ^= 1u << s;
-            form(U, U.k0 - 1 + u, stage0 + (size_t)s * stage_bytes, ring0 + (size_t)(u & (RING - 1)) * rplane_bytes);
+            if (u + 1 < P) tabs(U.k0 + u, (u + 1) % TSLOTS);
+            form(U, U.k0 - 1 + u, u % TSLOTS, stage0 + (size_t)s * stage_bytes,
+                 ring0 + (size_t)(u & (RING - 1)) * rplane_bytes);
             if (!__syncthreads_and(ok)) {
                 // copies this block started and has not waited for: plane u
                 // (whose wait gave up) and the ones issued after it
@@ -298,7 +341,7 @@ __device__ __forceinline__ bool zpass(const ZArgs &z, const Args &a, unsigned ch
             }
             if (threadIdx.x == 0 && u + S < P) issue(U, U.k0 - 1 + u + S, stage0 + (size_t)s * stage_bytes, &bars[s]);
             if (u >= 2) {
-                out(U, U.k0 + u - 2, ring0 + (size_t)((u - 2) & (RING - 1)) * rplane_bytes,
+                out(U, U.k0 + u - 2, (u - 1) % TSLOTS, ring0 + (size_t)((u - 2) & (RING - 1)) * rplane_bytes,
                     ring0 + (size_t)((u - 1) & (RING - 1)) * rplane_bytes,
                     ring0 + (size_t)(u & (RING - 1)) * rplane_bytes);
             }
@@ -363,32 +406,52 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         return __ldg(invt + mm * 9 + axis_class(j, ny) * 3 + axis_class(i, nx));
     };
 
+    // per-plane tables in shared memory (see zpass): slot s holds a plane's
+    // nine class rows (27 entries each) and then its nine Jacobi values, in
+    // FP64 (tab64) and FP32 (tab32)
+    double *tab64 = reinterpret_cast<double *>(smem + 128);
+    float *tab32 = reinterpret_cast<float *>(smem + 128 + r128(TSLOTS * TROW * 8));
+    auto tabs = [&](int m, int slot) {
+        const int mm = m < 0 ? 0 : (m >= nz ? nz - 1 : m);
+        for (int e = threadIdx.x; e < TROW; e += blockDim.x) {
+            const size_t src = e < 243 ? (size_t)mm * 243 + e : (size_t)mm * 9 + (e - 243);
+            tab64[slot * TROW + e] = e < 243 ? __ldg(st.table + src) : __ldg(z.inv64 + src);
+            tab32[slot * TROW + e] = e < 243 ? __ldg(st.table32 + src) : __ldg(z.inv32 + src);
+        }
+    };
+    auto tabT = [&](int slot) -> const T * {
+        if constexpr (sizeof(T) == 8) return tab64 + slot * TROW;
+        else return tab32 + slot * TROW;
+    };
+
     // ---- residual pass: r = b - A x (FP64), partials r.z, r.r, r64.r64 ----------
     auto residual = [&](double (&acc)[3]) -> bool {
         auto issue = [&](const Unit &U, int m, unsigned char *stg, uint64_t *bar) {
             mbar_expect_tx(bar, (unsigned)(L::ELEMS * 8));
             tma_load_3d(stg, tm_x, bar, U.x0 - HX, U.y0 - 1, m);
         };
-        auto form = [&](const Unit &, int, unsigned char *stg, unsigned char *rp) {
+        auto form = [&](const Unit &, int, int, unsigned char *stg, unsigned char *rp) {
             const double2 *src = reinterpret_cast<const double2 *>(stg);
             double2 *dst = reinterpret_cast<double2 *>(rp);
             for (int e = threadIdx.x; e < L::ELEMS / 2; e += blockDim.x) dst[e] = src[e];
         };
-        auto out = [&](const Unit &U, int k, unsigned char *lo, unsigned char *mid, unsigned char *hi) {
+        auto out = [&](const Unit &U, int k, int ts, unsigned char *lo, unsigned char *mid, unsigned char *hi) {
             const int j = U.y0 + w, i0 = U.x0 + 4 * lane;
             if (j >= ny) return;                     // warp-uniform
+            const double *ct = tab64 + ts * TROW;
             const V4<double> ax = apply27<double, W>(st, reinterpret_cast<const double *>(lo),
                                                      reinterpret_cast<const double *>(mid),
-                                                     reinterpret_cast<const double *>(hi), k, i0, j, w, lane);
+                                                     reinterpret_cast<const double *>(hi), ct, i0, j, w, lane);
             if (i0 >= nx) return;
             const size_t g0 = (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * k);
+            const T *iv = tabT(ts) + 243 + axis_class(j, ny) * 3;
             V4<T> rv;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const double bb = a.b ? a.b[g0 + e] : st.alpha * a.vstar[g0 + e];
                 const double r64 = bb - ax.v[e];
                 const T rt = (T)r64;
-                const T zz = pre ? mul_rn(inv_at(k, i0 + e, j), rt) : rt;
+                const T zz = pre ? mul_rn(iv[axis_class(i0 + e, nx)], rt) : rt;
                 rv.v[e] = rt;
                 acc[0] += (double)rt * (double)zz;
                 acc[1] += (double)rt * (double)rt;
@@ -396,7 +459,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
             }
             st4(r + g0, rv);
         };
-        return zpass<W, S>(z, a, smem, L::STAGE, L::RPLANE, pp, issue, form, out);
+        return zpass<W, S>(z, a, smem, L::TABS, L::STAGE, L::RPLANE, pp, issue, tabs, form, out);
     };
 
     // ---- Q pass: p = r / diag + beta p_old, A p, p.Ap ------------------------------
@@ -408,8 +471,9 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
             tma_load_3d(stg, tm_r, bar, U.x0 - HX, U.y0 - 1, m);
             if (!first) tma_load_3d(stg + L::ARR, mp, bar, U.x0 - HX, U.y0 - 1, m);
         };
-        auto form = [&](const Unit &U, int m, unsigned char *stg, unsigned char *rp) {
+        auto form = [&](const Unit &U, int m, int ts, unsigned char *stg, unsigned char *rp) {
             const T *rs = reinterpret_cast<const T *>(stg);
+            const T *itab = tabT(ts) + 243;
             const T *ps = reinterpret_cast<const T *>(stg + L::ARR);
             T *dst = reinterpret_cast<T *>(rp);
             const bool own_plane = m >= U.k0 && m < U.k1;
@@ -422,12 +486,13 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
                 V4<T> po = {{T(0), T(0), T(0), T(0)}};
                 if (!first) po = ld4(ps + o);
                 // away from the x faces the four cells share one class
+                const T *irow = itab + axis_class(j, ny) * 3;
                 T iv[4];
                 if (i > 0 && i + 3 < nx - 1) {
-                    iv[0] = iv[1] = iv[2] = iv[3] = inv_at(m, i + 1, j);
+                    iv[0] = iv[1] = iv[2] = iv[3] = irow[1];
                 } else {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) iv[q] = inv_at(m, i + q, j);
+                    for (int q = 0; q < 4; ++q) iv[q] = irow[axis_class(i + q, nx)];
                 }
                 V4<T> pv;
 #pragma unroll
@@ -440,12 +505,12 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
                     st4(pw + (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * m), pv);
             }
         };
-        auto out = [&](const Unit &U, int k, unsigned char *lo, unsigned char *mid, unsigned char *hi) {
+        auto out = [&](const Unit &U, int k, int ts, unsigned char *lo, unsigned char *mid, unsigned char *hi) {
             const int j = U.y0 + w, i0 = U.x0 + 4 * lane;
             if (j >= ny) return;
             const T *pm = reinterpret_cast<const T *>(mid);
             const V4<T> ap = apply27<T, W>(st, reinterpret_cast<const T *>(lo), pm, reinterpret_cast<const T *>(hi),
-                                           k, i0, j, w, lane);
+                                           tabT(ts), i0, j, w, lane);
             if (i0 >= nx) return;
             const size_t g0 = (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * k);
             st4(apb + g0, ap);
@@ -453,7 +518,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
 #pragma unroll
             for (int e = 0; e < 4; ++e) q1 += (double)pc.v[e] * (double)ap.v[e];
         };
-        return zpass<W, S>(z, a, smem, L::STAGE, L::RPLANE, pp, issue, form, out);
+        return zpass<W, S>(z, a, smem, L::TABS, L::STAGE, L::RPLANE, pp, issue, tabs, form, out);
     };
 
     // ---- U pass: x += alpha p, r -= alpha A p; r.z, r.r (z formed, not stored) -----
@@ -480,9 +545,10 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
                 const unsigned q = q0 + u * step;
                 if (q >= groups) continue;
                 const size_t g0 = (size_t)q << 2;
-                const unsigned t = q / gx;
+                const unsigned t = z.by_gx.div(q);
                 const int i0 = (int)(q - t * gx) << 2;
-                const int k = (int)(t / (unsigned)ny), j = (int)(t - (unsigned)k * (unsigned)ny);
+                const unsigned kk = z.by_ny.div(t);
+                const int k = (int)kk, j = (int)(t - kk * (unsigned)ny);
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     xv[u].v[e] += alpha * (double)pv[u].v[e];
@@ -612,6 +678,18 @@ static int grid_of(const Variant &var) {
     return sms * per;
 }
 
+// The multiply-shift constants of FastDiv for divisor d >= 1.
+static FastDiv fastdiv(uint32_t d) {
+    FastDiv f{d, 0u, 0u};
+    if (d > 1) {
+        uint32_t l = 0;
+        while ((1ull << l) < d) ++l;
+        f.l = l;
+        f.m = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+    }
+    return f;
+}
+
 typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -710,6 +788,8 @@ extern "C" int mbk_zcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
     z.maps = reinterpret_cast<const CUtensorMap *>(p->zc_maps) + 4 * p->zc_variant;
     z.tiles_x = (nx + TX - 1) / TX;
     z.tiles_y = (ny + var.warps - 1) / var.warps;
+    z.by_gx = fastdiv((uint32_t)(nx / 4));
+    z.by_ny = fastdiv((uint32_t)ny);
     {
         long long best = -1;
         int bc = 1;
