@@ -295,13 +295,16 @@ __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, 
 // timed out (the status word is set).
 //
 // Plane v of a unit (plane k0 - 1 + v) has its coefficient rows and Jacobi
-// values in table slot v % 4: loaded (tabs(m, slot)) in step v - 1 (the
-// prologue for v = 0) before that step's barrier, read by the form of step v
-// and the output of step v + 1, and rewritten in step v + 3 -- after the
-// barrier of step v + 2, which every reader of step v + 1 has passed.
+// values in table slot v % 4: read from global memory into registers
+// (tabs.fetch) in step v - 2, stored to the slot (tabs.put) in step v - 1
+// before that step's barrier (the prologue does both for v = 0 and fetches
+// v = 1), read by the form of step v and the output of step v + 1, and
+// rewritten in step v + 3 -- after the barrier of step v + 2, which every
+// reader of step v + 1 has passed.  The fetch one step ahead keeps the
+// global load's latency off the path to the barrier.
 template <int W, int S, typename IssueF, typename TabF, typename FormF, typename OutF>
 __device__ __forceinline__ bool zpass(const ZArgs &z, const Args &a, unsigned char *smem, int tabs_bytes,
-                                      int stage_bytes, int rplane_bytes, Pipe &pp, IssueF issue, TabF tabs,
+                                      int stage_bytes, int rplane_bytes, Pipe &pp, IssueF issue, TabF &tabs,
                                       FormF form, OutF out) {
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     unsigned char *stage0 = smem + 128 + tabs_bytes;
@@ -315,14 +318,17 @@ __device__ __forceinline__ bool zpass(const ZArgs &z, const Args &a, unsigned ch
             fence_proxy_async();
             for (int u = 0; u < S && u < P; ++u) issue(U, U.k0 - 1 + u, stage0 + (size_t)u * stage_bytes, &bars[u]);
         }
-        tabs(U.k0 - 1, 0);
+        tabs.fetch(U.k0 - 1);
+        tabs.put(0);
+        if (P > 1) tabs.fetch(U.k0);
         __syncthreads();
         for (int u = 0; u < P; ++u) {
             const int s = u % S;
             const unsigned par = (pp.phase >> s) & 1u;
             const bool ok = mbar_wait(&bars[s], par);
             pp.phase ^= 1u << s;
-            if (u + 1 < P) tabs(U.k0 + u, (u + 1) % TSLOTS);
+            if (u + 1 < P) tabs.put((u + 1) % TSLOTS);
+            if (u + 2 < P) tabs.fetch(U.k0 + u + 1);
             form(U, U.k0 - 1 + u, u % TSLOTS, stage0 + (size_t)s * stage_bytes,
                  ring0 + (size_t)(u & (RING - 1)) * rplane_bytes);
             if (!__syncthreads_and(ok)) {
@@ -350,6 +356,44 @@ __device__ __forceinline__ bool zpass(const ZArgs &z, const Args &a, unsigned ch
     }
     return true;
 }
+
+// A plane's class rows and Jacobi values (TROW entries per precision), each
+// thread holding the entries e = threadIdx.x + NT i between fetch and put.
+template <int NT>
+struct Tabs {
+    static constexpr int PER = (TROW + NT - 1) / NT;
+    double *tab64;
+    float *tab32;
+    const double *table;
+    const float *table32;
+    const double *inv64;
+    const float *inv32;
+    int nz;
+    double h64[PER];
+    float h32[PER];
+    __device__ __forceinline__ void fetch(int m) {
+        const int mm = m < 0 ? 0 : (m >= nz ? nz - 1 : m);
+#pragma unroll
+        for (int i = 0; i < PER; ++i) {
+            const int e = threadIdx.x + NT * i;
+            if (e < TROW) {
+                const size_t src = e < 243 ? (size_t)mm * 243 + e : (size_t)mm * 9 + (e - 243);
+                h64[i] = e < 243 ? __ldg(table + src) : __ldg(inv64 + src);
+                h32[i] = e < 243 ? __ldg(table32 + src) : __ldg(inv32 + src);
+            }
+        }
+    }
+    __device__ __forceinline__ void put(int slot) {
+#pragma unroll
+        for (int i = 0; i < PER; ++i) {
+            const int e = threadIdx.x + NT * i;
+            if (e < TROW) {
+                tab64[slot * TROW + e] = h64[i];
+                tab32[slot * TROW + e] = h32[i];
+            }
+        }
+    }
+};
 
 // ---- the solve ----------------------------------------------------------------
 
@@ -398,27 +442,12 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
     Pipe pp{0u};
     int red = 0;
 
-    // Jacobi 1/diag of a staged or tile cell (i, j) of plane m (clamped into
-    // the grid: values outside it are zero and multiply whatever it returns)
-    auto inv_at = [&](int m, int i, int j) -> T {
-        if (!pre) return T(1);
-        const int mm = m < 0 ? 0 : (m >= nz ? nz - 1 : m);
-        return __ldg(invt + mm * 9 + axis_class(j, ny) * 3 + axis_class(i, nx));
-    };
-
     // per-plane tables in shared memory (see zpass): slot s holds a plane's
     // nine class rows (27 entries each) and then its nine Jacobi values, in
     // FP64 (tab64) and FP32 (tab32)
     double *tab64 = reinterpret_cast<double *>(smem + 128);
     float *tab32 = reinterpret_cast<float *>(smem + 128 + r128(TSLOTS * TROW * 8));
-    auto tabs = [&](int m, int slot) {
-        const int mm = m < 0 ? 0 : (m >= nz ? nz - 1 : m);
-        for (int e = threadIdx.x; e < TROW; e += blockDim.x) {
-            const size_t src = e < 243 ? (size_t)mm * 243 + e : (size_t)mm * 9 + (e - 243);
-            tab64[slot * TROW + e] = e < 243 ? __ldg(st.table + src) : __ldg(z.inv64 + src);
-            tab32[slot * TROW + e] = e < 243 ? __ldg(st.table32 + src) : __ldg(z.inv32 + src);
-        }
-    };
+    Tabs<32 * W> tabs{tab64, tab32, st.table, st.table32, z.inv64, z.inv32, nz};
     auto tabT = [&](int slot) -> const T * {
         if constexpr (sizeof(T) == 8) return tab64 + slot * TROW;
         else return tab32 + slot * TROW;
@@ -549,12 +578,22 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
                 const int i0 = (int)(q - t * gx) << 2;
                 const unsigned kk = z.by_ny.div(t);
                 const int k = (int)kk, j = (int)(t - kk * (unsigned)ny);
+                // Jacobi values of the group: the row's interior class, and
+                // its face classes for the first / last cell of an x-row
+                T iv[4] = {T(1), T(1), T(1), T(1)};
+                if (pre) {
+                    const T *irow = invt + k * 9 + axis_class(j, ny) * 3;
+                    const T lo = __ldg(irow), mi = __ldg(irow + 1), hi = __ldg(irow + 2);
+                    iv[0] = i0 == 0 ? lo : mi;
+                    iv[1] = iv[2] = mi;
+                    iv[3] = i0 + 3 == nx - 1 ? hi : mi;
+                }
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     xv[u].v[e] += alpha * (double)pv[u].v[e];
                     const T rn = fma(-al, av[u].v[e], rv[u].v[e]);
                     rv[u].v[e] = rn;
-                    const T zz = pre ? mul_rn(inv_at(k, i0 + e, j), rn) : rn;
+                    const T zz = pre ? mul_rn(iv[e], rn) : rn;
                     u2[0] += (double)zz * (double)rn;
                     u2[1] += (double)rn * (double)rn;
                 }
