@@ -915,7 +915,9 @@ static int ode_autotune(mb_monodomain *m) {
     }
     int n64, n32;
     ode_rows(m->desc.model, m->desc.precision, &n64, &n32);
-    const uint32_t nt = m->n_active < (1u << 20) ? m->n_active : (1u << 20);
+    /* a sample of up to 4 M cells: launch shapes rank differently on a few
+     * waves of blocks than on the tens of waves of a large tissue */
+    const uint32_t nt = m->n_active < (1u << 22) ? m->n_active : (1u << 22);
     double *s64 = NULL, *vs = NULL;
     float *s32 = NULL;
     int rc = MB_OK;
