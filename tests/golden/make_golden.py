@@ -1,32 +1,41 @@
 """Generate the golden fixtures of the parity tests by running the reference
 MonoAlg3D CPU path (FP64, OpenMP), built from its own sources into
-oracle/_ref/ by oracle/ref/Makefile.
+oracle/_ref/ by oracle/ref/Makefile, through oracle/ref/run_reference.py.
 
-    python tests/golden/make_golden.py            # writes tests/golden/*.npz
+    python tests/golden/make_golden.py [case ...]     # writes tests/golden/<case>.npz
 
-Each case writes an ini file, runs oracle/_ref/bin/MonoAlg3D with the binary
-V writer (save_as_text_or_binary, binary=true: centre, half sizes and V as
-doubles per active cell), maps the cells to grid order by their centres and
-stores V every `print_rate` steps plus the CG iterations and error of every
-step from the solver log (and, for the ECG case, the reference's ecg.txt).  Runs only where the reference tree is mounted; the
-fixtures are committed and the tests read only them.
+Each case runs the reference binary with V dumped every `PRINT_RATE` steps
+(centre, half sizes and V as doubles per active cell, mapped to grid order by
+the centres) and keeps V at those steps, the CG iterations and error of every
+step from the solver log and, for the ECG case, the reference's ecg.txt.
+Inputs the stock plugins cannot express (removed-cell masks, fibres rotating
+through the thickness, z-layered ToRORd cell types) go through the adapter
+plugins of oracle/ref/adapters.c.  Runs only where the reference tree was
+built; the fixtures are committed and the tests read only them.
 """
 from __future__ import annotations
 
 import json
 import os
-import re
-import subprocess
 import sys
-import tempfile
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.path.join(REPO, "oracle", "_ref")
-BIN = os.path.join(REF, "bin", "MonoAlg3D")
-LIBS = os.path.join(REF, "shared_libs")
+sys.path.insert(0, os.path.join(REPO, "oracle", "ref"))
+import run_reference as rr  # noqa: E402
+
+DX = 100.0
+DT = 0.02
+PRINT_RATE = 50
+SEED_MASK = 1001
+
+
+def _philox_mask(n: int, phi: float) -> np.ndarray:
+    """i.i.d. Bernoulli removal of a fraction phi, numpy's Philox keyed by the seed."""
+    return (np.random.Generator(np.random.Philox(SEED_MASK)).random(n) >= phi).astype(np.uint8)
+
 
 # Each case: geometry (cells), model, assembly and simulation length.
 CASES = {
@@ -45,139 +54,60 @@ CASES = {
     "tt2006_ecg": dict(nx=32, ny=16, nz=3, model="tt2006", assembly="homogeneous", sim_ms=30.0,
                        ecg=dict(leads=[[-500.0, 800.0, 150.0], [3700.0, 800.0, 150.0], [1600.0, -400.0, 150.0]],
                                 sigma_b=1.0, calc_rate=5)),
+    # the precision configuration's tissue kind: ToRORd endo, fibres along x
+    # (sigma_l 0.2, sigma_t 0.05 S/m), 20 % of the volumes removed (3-D mask)
+    "torord_fibrosis_aniso": dict(nx=32, ny=16, nz=4, model="torord", assembly="anisotropic", fibre_deg=0.0,
+                                  sigma_l=0.0002, sigma_t=0.00005, fibrosis=0.2, sim_ms=12.0),
+    # the scale configuration's tissue kind: ToRORd in z-thirds endo / mid /
+    # epi, fibres rotating from +60 to -60 degrees through the thickness
+    # (sigma_l 0.2, sigma_t 0.04 S/m, 27-point rows)
+    "torord_rotating_transmural": dict(nx=32, ny=16, nz=6, model="torord", assembly="anisotropic",
+                                       fibre_rotate=(60.0, -60.0), sigma_l=0.0002, sigma_t=0.00004,
+                                       z_thirds=True, sim_ms=12.0),
 }
 
-DX = 100.0
-DT = 0.02
-PRINT_RATE = 50
 
-
-def ini_text(case: dict, out_dir: str) -> str:
-    nx, ny, nz = case["nx"], case["ny"], case["nz"]
-    model_lib = {"tt2006": "libten_tusscher_2006.so", "torord": "libToRORd_fkatp_mixed_endo_mid_epi.so"}[case["model"]]
+def reference_case(case: dict) -> dict:
+    """The run_reference case of a fixture case."""
+    c = dict(nx=case["nx"], ny=case["ny"], nz=case["nz"], dx=DX, dt=DT, model=case["model"],
+             assembly=case["assembly"], sim_ms=case["sim_ms"])
     if case["assembly"] == "homogeneous":
-        assembly = ("main_function=homogeneous_sigma_assembly_matrix\n"
-                    "sigma_x=0.00013\nsigma_y=0.00013\nsigma_z=0.00013\n")
+        c["sigma"] = (0.00013, 0.00013, 0.00013)
     else:
-        th = np.deg2rad(case["fibre_deg"])
-        assembly = ("main_function=anisotropic_sigma_assembly_matrix\n"
-                    "sigma_l=0.0002\nsigma_t=0.00005\nsigma_n=0.00005\n"
-                    f"f=[{float(np.cos(th))!r},{float(np.sin(th))!r},0.0]\n")
-    extra = ""
-    if case.get("ecg"):
-        e = case["ecg"]
-        leads = "".join(f"lead{i + 1}={x!r},{y!r},{z!r}\n" for i, (x, y, z) in enumerate(e["leads"]))
-        extra += ("[calc_ecg]\nmain_function=pseudo_bidomain\ninit_function=init_pseudo_bidomain\n"
-                  f"end_function=end_pseudo_bidomain\ncalc_rate={e['calc_rate']}\n{leads}sigma_b={e['sigma_b']!r}\n"
-                  f"use_gpu=no\nlibrary_file={LIBS}/libdefault_calc_ecg.so\n\n")
+        c.update(sigma_l=case.get("sigma_l", 0.0002), sigma_t=case.get("sigma_t", 0.00005))
+        c["sigma_n"] = c["sigma_t"]
+        if case.get("fibre_rotate"):
+            c["fibre_rotate"] = tuple(case["fibre_rotate"])
+        else:
+            c["fibre_deg"] = case["fibre_deg"]
+    if case.get("fibrosis"):
+        c["mask"] = _philox_mask(case["nx"] * case["ny"] * case["nz"], case["fibrosis"])
     if case.get("extra_data"):
-        extra += ("[extra_data]\nmain_function=set_extra_data_mixed_torord_fkatp_epi_mid_endo\n"
-                  f"library_file={LIBS}/libdefault_extra_data.so\n")
-    return f"""[main]
-num_threads=4
-dt_pde={DT}
-simulation_time={case['sim_ms']}
-abort_on_no_activity=false
-use_adaptivity=false
-
-[update_monodomain]
-main_function=update_monodomain_default
-library_file={LIBS}/libdefault_update_monodomain.so
-
-[save_result]
-print_rate=1
-output_dir={out_dir}
-main_function=save_as_text_or_binary
-binary=true
-file_prefix=V
-library_file={LIBS}/libdefault_save_mesh.so
-
-[assembly_matrix]
-init_function=set_initial_conditions_fvm
-{assembly}library_file={LIBS}/libdefault_matrix_assembly.so
-
-[linear_system_solver]
-tolerance=1e-16
-use_preconditioner=yes
-max_iterations=200
-library_file={LIBS}/libdefault_linear_system_solver.so
-use_gpu=no
-main_function=conjugate_gradient
-init_function=init_conjugate_gradient
-end_function=end_conjugate_gradient
-
-[domain]
-name=Cuboid Mesh
-start_dx={DX}
-start_dy={DX}
-start_dz={DX}
-side_length_x={nx * DX}
-side_length_y={ny * DX}
-side_length_z={nz * DX}
-main_function=initialize_grid_with_cuboid_mesh
-library_file={LIBS}/libdefault_domains.so
-
-[ode_solver]
-dt={DT}
-use_gpu=no
-gpu_id=0
-library_file={LIBS}/{model_lib}
-
-{extra}
-[stim_plain]
-start = 0.0
-duration = 2.0
-current = -53.0
-x_limit = 500.0
-main_function=stim_if_x_less_than
-library_file={LIBS}/libdefault_stimuli.so
-"""
-
-
-def read_bin(path: str, nx: int, ny: int, nz: int) -> np.ndarray:
-    rec = np.fromfile(path, dtype=np.float64).reshape(-1, 7)
-    v = np.full(nx * ny * nz, np.nan)
-    i = np.floor(rec[:, 0] / DX).astype(int)
-    j = np.floor(rec[:, 1] / DX).astype(int)
-    k = np.floor(rec[:, 2] / DX).astype(int)
-    v[i + nx * (j + ny * k)] = rec[:, 6]
-    return v
+        c["celltype"] = "x_45_25_30"
+    if case.get("z_thirds"):
+        c["celltype"] = "z_thirds"
+    if case.get("ecg"):
+        c["ecg"] = case["ecg"]
+    return c
 
 
 def run_case(name: str, case: dict) -> dict:
-    with tempfile.TemporaryDirectory() as tmp:
-        out_dir = os.path.join(tmp, "out")
-        ini = os.path.join(tmp, f"{name}.ini")
-        with open(ini, "w") as f:
-            f.write(ini_text(case, out_dir))
-        log = subprocess.run([BIN, "-c", ini, "-p", "1"], capture_output=True, text=True, check=True).stdout
-        its, errs = [], []
-        for m in re.finditer(r"t = ([0-9.]+), Iterations = (\d+), Error Norm = ([0-9.eE+-]+)", log):
-            its.append(int(m.group(2)))
-            errs.append(float(m.group(3)))
-        counts = sorted(int(re.match(r"V_it_(\d+)\.bin$", f).group(1))
-                        for f in os.listdir(out_dir) if re.match(r"V_it_\d+\.bin$", f))
-        counts = [c for c in counts if c % PRINT_RATE == 0]
-        V = np.stack([read_bin(os.path.join(out_dir, f"V_it_{c}.bin"), case["nx"], case["ny"], case["nz"])
-                      for c in counts])
-        res = dict(V=V, counts=np.array(counts), its=np.array(its), errors=np.array(errs),
-                   config=json.dumps(dict(case, dx=DX, dt=DT, print_rate=PRINT_RATE)))
-        if case.get("ecg"):
-            # ecg.txt: time and one value per lead per line, "%lf" (ecg.c:286-306)
-            rows = np.loadtxt(os.path.join(out_dir, "ecg.txt"), ndmin=2)
-            res["ecg_t"] = rows[:, 0]
-            res["ecg"] = rows[:, 1:]
+    r = rr.run_case(reference_case(case), threads=4, dumps_every=PRINT_RATE)
+    res = dict(V=r["V"], counts=r["counts"], its=r["its"], errors=r["errors"],
+               config=json.dumps(dict(case, dx=DX, dt=DT, print_rate=PRINT_RATE)))
+    if case.get("ecg"):
+        res["ecg_t"] = r["ecg_t"]
+        res["ecg"] = r["ecg"]
     return res
 
 
-def main(names=None):
-    if not os.path.exists(BIN):
-        sys.exit(f"{BIN} not built: run `make -C oracle/ref` first")
+def main(names=None, out_dir=HERE):
+    if not rr.available():
+        sys.exit(f"{rr.BIN} and the adapter plugins are not built: run `make -C oracle/ref` first")
     for name in names or CASES:
         res = run_case(name, CASES[name])
-        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **res)
-        print(f"{name}: {len(res['its'])} steps, {len(res['counts'])} dumps, "
-              f"mean CG its {res['its'].mean():.2f}")
+        np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **res)
+        print(f"{name}: {len(res['its'])} steps, {len(res['counts'])} dumps, mean CG its {res['its'].mean():.2f}")
 
 
 if __name__ == "__main__":

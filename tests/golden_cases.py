@@ -8,7 +8,8 @@ import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASE_NAMES = ["tt2006_cuboid", "torord_endo_cuboid", "torord_transmural_cuboid", "tt2006_aniso_x",
-              "tt2006_aniso_30"]
+              "tt2006_aniso_30", "torord_fibrosis_aniso", "torord_rotating_transmural"]
+SEED_MASK = 1001
 
 
 def load(name: str) -> dict:
@@ -34,12 +35,24 @@ def tissue_kwargs(cfg: dict) -> dict:
     kw = dict(dx=cfg["dx"], dy=cfg["dx"], dz=cfg["dx"], dt_pde=cfg["dt"], model=cfg["model"],
               cg_tolerance=1e-16, cg_max_iterations=200, use_preconditioner=True,
               stims=[Stim(kind="x_less_than", start=0.0, duration=2.0, current=-53.0, x_limit=500.0)])
+    nx, ny, nz = cfg["nx"], cfg["ny"], cfg["nz"]
     if cfg["assembly"] == "homogeneous":
         kw.update(assembly="homogeneous", sigma=(0.00013, 0.00013, 0.00013))
     else:
-        th = np.deg2rad(cfg["fibre_deg"])
-        kw.update(assembly="anisotropic", sigma_l=0.0002, sigma_t=0.00005, sigma_n=0.00005,
-                  fibre_angle_z=np.full(cfg["nz"], th))
+        st = cfg.get("sigma_t", 0.00005)
+        kw.update(assembly="anisotropic", sigma_l=cfg.get("sigma_l", 0.0002), sigma_t=st, sigma_n=st)
+        if cfg.get("fibre_rotate"):
+            # theta(k) = bottom + (top - bottom) (k + 1/2) / nz at the cell centres
+            b, t = cfg["fibre_rotate"]
+            kw["fibre_angle_z"] = np.deg2rad(b + (t - b) * ((np.arange(nz) + 0.5) / nz))
+        else:
+            kw["fibre_angle_z"] = np.full(nz, np.deg2rad(cfg["fibre_deg"]))
+    if cfg.get("fibrosis"):
+        kw["active"] = (np.random.Generator(np.random.Philox(SEED_MASK)).random(nx * ny * nz)
+                        >= cfg["fibrosis"]).astype(np.uint8)
     if cfg.get("extra_data"):
-        kw["celltype"] = transmural_celltype(cfg["nx"], cfg["ny"], cfg["nz"], cfg["dx"])
+        kw["celltype"] = transmural_celltype(nx, ny, nz, cfg["dx"])
+    if cfg.get("z_thirds"):
+        ct = np.minimum(2, (3 * np.arange(nz)) // nz).astype(np.uint8)
+        kw["celltype"] = np.broadcast_to(ct[:, None, None], (nz, ny, nx)).reshape(-1).copy()
     return kw
