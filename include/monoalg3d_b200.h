@@ -393,10 +393,13 @@ void mb_csr_destroy(mb_csr *a);
  * DEVICE pointers supplied by the caller, x holds the initial guess and
  * receives the solution, and the work vectors live in a fixed 16 MiB + 64 KiB
  * device array inside this library (held on every GPU that loads it until
- * exit).  Nothing is allocated or freed.  n is limited to 524288 rows;
- * larger systems are rejected with MB_ERR_ARG.  The array's device address is
- * looked up on the first call made while a device is current: make that
- * first call before any stream capture on the device.  All calls share the
+ * exit; it is placed on a device, with the library's module, at the first call
+ * made there, which may synchronise the device: make one warm-up call at
+ * initialisation).  Nothing is allocated or freed.  n is limited to 524288
+ * rows; larger systems are rejected with MB_ERR_ARG.  The array's device
+ * address is looked up on that first call: make it before any stream capture
+ * on the device.  Each call waits on its stream (it reads the convergence
+ * flag back), which must belong to the current device.  All calls share the
  * array, so calls whose work overlaps on the GPU race and must be serialised
  * by the caller.  stream may be NULL (legacy default stream).  Returns the
  * iteration count and the final r.r in host memory.                          */

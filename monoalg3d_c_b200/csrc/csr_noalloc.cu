@@ -14,10 +14,15 @@
 // Its work vectors (r, p, q, 1/diag), the block partial sums and the CG control
 // block live in one file-scope device array, mb_noalloc_scratch, of
 // MB_NOALLOC_SCRATCH_BYTES (16 MiB + 64 KiB).  Every GPU that loads this library
-// holds that array until the process exits.  The device address of the array
-// is obtained once per device with cudaGetSymbolAddress, on the first call
-// made while that device is current; make that first call before any stream
-// capture on the device.  All calls share the array and it keeps the last
+// holds that array until the process exits; under CUDA's lazy module loading
+// the array (and the module) are placed on a device at the first call made
+// there, which may synchronise the device -- a caller with a fixed budget or
+// a real-time loop makes one warm-up call at initialisation.  The device
+// address of the array is obtained once per device with
+// cudaGetSymbolAddress, on that first call; make it before any stream
+// capture on the device.  Each call waits on its stream while it runs (it
+// reads the convergence flag back to the host), and the stream must belong
+// to the current device.  All calls share the array and it keeps the last
 // call's contents: each call rewrites the control block (the only part that
 // must start from known values) before launching, and every vector is written
 // before it is read.  Calls whose work overlaps on the GPU -- on two streams,
@@ -37,6 +42,8 @@
 #define MB_NOALLOC_SCRATCH_BYTES ((size_t)MB_NOALLOC_HEADER_BYTES + 4ull * MB_NOALLOC_MAX_ROWS * sizeof(double))
 
 static __device__ __align__(256) unsigned char mb_noalloc_scratch[MB_NOALLOC_SCRATCH_BYTES];
+
+static_assert(sizeof(mb_ctrl) <= 4096, "the control block must fit before the partial sums");
 
 namespace {
 
@@ -92,10 +99,20 @@ extern "C" int mb_csr_conjugate_gradient_noalloc(int32_t n, const int32_t *row_p
     int rc = scratch_for_current_device(&base, err, sizeof err);
     if (rc) return mb_noalloc_set_error(rc, err);
     cudaStream_t s = (cudaStream_t)stream;
+    if (s) {
+        int sdev = -1, cur = -1;
+        if (cudaStreamGetDevice(s, &sdev) != cudaSuccess || cudaGetDevice(&cur) != cudaSuccess || sdev != cur) {
+            cudaGetLastError();
+            return mb_noalloc_set_error(MB_ERR_ARG, "mb_csr_conjugate_gradient_noalloc: the stream does not "
+                                                    "belong to the current device");
+        }
+    }
 
     // layout: [control block][partials][r][p][q][1/diag]
     int gb = (n + 255) / 256;
     if (gb > mbk_max_grid_blocks()) gb = mbk_max_grid_blocks();
+    if ((size_t)gb * 3 * sizeof(double) > MB_NOALLOC_HEADER_BYTES - 4096)
+        return mb_noalloc_set_error(MB_ERR_ARG, "mb_csr_conjugate_gradient_noalloc: partial sums exceed the header");
     mb_ctrl *ctrl = (mb_ctrl *)base;
     double *partials = (double *)(base + 4096);
     double *vec = (double *)(base + MB_NOALLOC_HEADER_BYTES);

@@ -993,11 +993,11 @@ static int cap_post(mb_monodomain *m, int in_body) {
     return mbk_step_end(m->d_ctrl, m->desc.dt_pde, m->desc.dt_ode, m->num_steps, m->d_log, m->log_len, m->stream);
 }
 
-static unsigned long long g_cond_handle;
-
-static int cap_body(mb_monodomain *m, int in_body) {
-    (void)in_body;
-    return mbk_cg_body(&m->st, &m->cg, m->d_ctrl, g_cond_handle, 1, m->stream);
+/* The CG body captured into the conditional node's body graph, given the
+ * node's handle (per tissue, passed down: tissues created concurrently from
+ * several host threads each capture their own). */
+static int cap_body(mb_monodomain *m, unsigned long long cond) {
+    return mbk_cg_body(&m->st, &m->cg, m->d_ctrl, cond, 1, m->stream);
 }
 
 static int capture_graph(mb_monodomain *m, capture_fn fn, cudaGraph_t *out) {
@@ -1032,9 +1032,8 @@ static int build_loop_graph(mb_monodomain *m, capture_fn pre, capture_fn post, c
     cp.conditional.size = 1;
     CK(cudaGraphAddNode(&ncond, g, &npre, 1, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
-    g_cond_handle = (unsigned long long)h;
     CK(cudaStreamBeginCaptureToGraph(m->stream, body, NULL, NULL, 0, cudaStreamCaptureModeThreadLocal));
-    int e = cap_body(m, 1);
+    int e = cap_body(m, (unsigned long long)h);
     cudaGraph_t body_out = NULL;
     cudaError_t ee = cudaStreamEndCapture(m->stream, &body_out);
     if (e) return set_err(MB_ERR_CUDA, "CG body capture failed: %s", cudaGetErrorString((cudaError_t)e));

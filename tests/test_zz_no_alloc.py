@@ -12,9 +12,12 @@ a symmetric positive definite system on the device with torch, solves it
 twice in a row through the C ABI with the allocation-free entry point, and
 checks each solution and iteration count against the allocating entry point
 mb_csr_conjugate_gradient on the same system (same kernels, so the results
-agree to rounding; the tolerance allows 1e-12 relative).  It also checks that
-a system above the scratch limit is rejected.  The file is named to be
-collected last and runs alone in a fresh process as well.
+agree to rounding; the tolerance allows 1e-12 relative).  After one warm-up
+call (the first call on a device places the library's fixed array there),
+the device's free memory is the same before and after the two calls: they
+allocate nothing.  It also checks that a system above the scratch limit is
+rejected.  The file is named to be collected last and runs alone in a fresh
+process as well.
 """
 import ctypes as C
 
@@ -64,24 +67,36 @@ def test_noalloc_matches_allocating_solver_twice():
     d_col = torch.from_numpy(col).to(dev)
     d_val = torch.from_numpy(val).to(dev)
 
-    for call in range(2):
-        b = rng.standard_normal(n)
-        x0 = rng.standard_normal(n) * 0.1
-        x_ref, its_ref, err_ref = csr_conjugate_gradient(row_ptr, col, val, b, x0, tolerance=1e-20,
-                                                         max_iterations=500, use_preconditioner=True)
-        d_b = torch.from_numpy(b).to(dev)
-        d_x = torch.from_numpy(x0.copy()).to(dev)
-        torch.cuda.synchronize()
+    def solve(d_b, d_x):
         its, err = C.c_uint32(), C.c_double()
         rc = _lib.lib.mb_csr_conjugate_gradient_noalloc(
             n, C.c_void_p(d_rp.data_ptr()), C.c_void_p(d_col.data_ptr()), C.c_void_p(d_val.data_ptr()),
             C.c_void_p(d_b.data_ptr()), C.c_void_p(d_x.data_ptr()), 1e-20, 500, 1, C.byref(its), C.byref(err),
             None)
         _lib.check(rc)
+        return its.value, err.value
+
+    # the references (the allocating solver) and every device buffer first
+    cases = []
+    for call in range(2):
+        b = rng.standard_normal(n)
+        x0 = rng.standard_normal(n) * 0.1
+        ref = csr_conjugate_gradient(row_ptr, col, val, b, x0, tolerance=1e-20, max_iterations=500,
+                                     use_preconditioner=True)
+        cases.append((b, ref, torch.from_numpy(b).to(dev), torch.from_numpy(x0.copy()).to(dev)))
+    warm_x = cases[0][3].clone()
+    solve(cases[0][2], warm_x)         # places the fixed array on the device
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(0)[0]
+    results = [solve(d_b, d_x) for (_, _, d_b, d_x) in cases]
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free_before, "the calls changed the device's free memory"
+
+    for call, ((b, (x_ref, its_ref, err_ref), _, d_x), (its, err)) in enumerate(zip(cases, results)):
         x = d_x.cpu().numpy()
-        assert its.value == its_ref, f"call {call}: {its.value} vs {its_ref} iterations"
+        assert its == its_ref, f"call {call}: {its} vs {its_ref} iterations"
         np.testing.assert_allclose(x, x_ref, rtol=1e-12, atol=1e-12 * np.abs(x_ref).max())
-        assert err.value == pytest.approx(err_ref, rel=1e-9, abs=1e-30)
+        assert err == pytest.approx(err_ref, rel=1e-9, abs=1e-30)
         # the solution really solves the system
         A = np.zeros(n)
         for r in range(n):
