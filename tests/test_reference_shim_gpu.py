@@ -3,11 +3,12 @@ oracle/_ref, built from its own sources) runs its own time loop twice on the
 same ini, once with its stock cell-model and linear-solver plugins and once
 with this library's reference-host plugins (monoalg3d_c_b200/shim: the
 same entry points, the ODE and CG work on the GPU) named in [ode_solver]
-and [linear_system_solver] library_file.  The V dumps (the reference's own
-save_as_text_or_binary writer) and the CG iteration counts of the two runs
-are compared.  Bar: V within 1e-8 relative (FP64), identical iteration
+and [linear_system_solver] library_file.  The V dumps (the binary layout of
+the reference's save_as_text_or_binary, every 10 steps) and the CG iteration
+counts of every step of the two runs are compared.  Bar: V within 1e-8 relative (FP64), identical iteration
 counts."""
 import os
+import re
 import subprocess
 import sys
 import tempfile
@@ -18,7 +19,9 @@ import pytest
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 sys.path.insert(0, os.path.join(HERE, "golden"))
+sys.path.insert(0, os.path.join(REPO, "oracle", "ref"))
 import make_golden as mg  # noqa: E402
+import run_reference as rr  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -28,29 +31,31 @@ MODEL_LIB = {"tt2006": "libten_tusscher_2006.so", "torord": "libToRORd_fkatp_mix
 
 
 def _run(case, shim):
+    """The reference binary on a fixture case (V dumped every 10 steps, the CG
+    log of every step), with its stock plugins or with the shim."""
     with tempfile.TemporaryDirectory() as tmp:
         out_dir = os.path.join(tmp, "out")
-        text = mg.ini_text(case, out_dir)
+        text = rr.ini_text(mg.reference_case(case), tmp, out_dir, dumps_every=10)
         if shim:
             lib = SHIM[case["model"]]
-            stock_model = f"library_file={mg.LIBS}/{MODEL_LIB[case['model']]}"
-            stock_solver = f"library_file={mg.LIBS}/libdefault_linear_system_solver.so"
+            stock_model = f"library_file={rr.LIBS}/{MODEL_LIB[case['model']]}"
+            stock_solver = f"library_file={rr.LIBS}/libdefault_linear_system_solver.so"
             assert stock_model in text and stock_solver in text
             text = text.replace(stock_model, f"library_file={lib}").replace(stock_solver, f"library_file={lib}")
         ini = os.path.join(tmp, "case.ini")
         with open(ini, "w") as f:
             f.write(text)
-        log = subprocess.run([mg.BIN, "-c", ini, "-p", "1"], capture_output=True, text=True, timeout=600)
+        log = subprocess.run([rr.BIN, "-c", ini], capture_output=True, text=True, timeout=600)
         assert log.returncode == 0, log.stdout[-2000:] + log.stderr[-2000:]
-        its = [int(m.group(2)) for m in mg.re.finditer(
+        its = [int(m.group(2)) for m in re.finditer(
             r"t = ([0-9.]+), Iterations = (\d+), Error Norm = ([0-9.eE+-]+)", log.stdout)]
-        files = sorted((int(mg.re.match(r"V_it_(\d+)\.bin$", f).group(1)), f)
-                       for f in os.listdir(out_dir) if mg.re.match(r"V_it_\d+\.bin$", f))
-        V = np.stack([mg.read_bin(os.path.join(out_dir, f), case["nx"], case["ny"], case["nz"]) for _, f in files])
+        files = sorted((int(re.match(r"V_it_(\d+)\.bin$", f).group(1)), f)
+                       for f in os.listdir(out_dir) if re.match(r"V_it_\d+\.bin$", f))
+        V = np.stack([rr.read_bin(os.path.join(out_dir, f), case["nx"], case["ny"], case["nz"]) for _, f in files])
         return np.array(its), V, [c for c, _ in files]
 
 
-@pytest.mark.skipif(not os.path.exists(mg.BIN), reason="the reference build (oracle/_ref) is not present")
+@pytest.mark.skipif(not rr.available(), reason="the reference build (oracle/_ref) is not present")
 @pytest.mark.parametrize("name", ["tt2006_cuboid", "torord_endo_cuboid", "tt2006_aniso_30"])
 def test_reference_binary_with_shim(name):
     case = mg.CASES[name]
