@@ -169,10 +169,22 @@ class ClockSampler:
 # bench's tuner picked that same kernel, else the field is null.
 #   (workload, cg kernel id) -> DRAM bytes (dram__bytes_read.sum +
 #   dram__bytes_write.sum) per active cell and CG iteration of one launch
-PROFILED_CG_TRAFFIC = {}
+PROFILED_CG_TRAFFIC = {
+    # k_zcg<1, 8, 3, 2> on the 0.72-scale slab (360x360x72, every vector
+    # larger than L2): 6.411 GB over 9.33 M cells x 15 iterations
+    ("slab_500x500x100_torord_rotating_fibres", 301): 45.8,
+}
 #   (workload, "mixed" | "fp64", ode variant) -> pipe utilisation and MUFU
 #   (XU pipe) warp instructions x 32 per cell-step of one launch
-PROFILED_ODE = {}
+PROFILED_ODE = {
+    # k_torord_mixed<0, 4> / k_torord_fp64<0, 3> on the 0.72-scale slab
+    ("slab_500x500x100_torord_rotating_fibres", "mixed", 3): {
+        "xu_pct": 43.6, "fma_pct": 28.8, "fp64_pct": 1.1, "dram_bytes_per_cell_step": 411.6,
+        "mufu_per_cell_step": 227.0},
+    ("slab_500x500x100_torord_rotating_fibres", "fp64", 2): {
+        "fp64_pipe_pct": 18.5, "xu_pct": 4.7, "issue_active_pct": 22.1, "fp64_ops_per_cell_step": 3910.0,
+        "mufu_per_cell_step": 248.3},
+}
 
 
 def measured_peaks():

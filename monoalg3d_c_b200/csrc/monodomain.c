@@ -915,9 +915,18 @@ static int ode_autotune(mb_monodomain *m) {
     }
     int n64, n32;
     ode_rows(m->desc.model, m->desc.precision, &n64, &n32);
-    /* a sample of up to 4 M cells: launch shapes rank differently on a few
-     * waves of blocks than on the tens of waves of a large tissue */
-    const uint32_t nt = m->n_active < (1u << 22) ? m->n_active : (1u << 22);
+    /* every cell where the scratch outputs fit in a quarter of the free
+     * device memory (launch shapes rank differently on a few waves of blocks
+     * than on the hundreds of waves of a large tissue), else 4 M cells */
+    uint32_t nt = m->n_active;
+    {
+        size_t fr = 0, tot = 0;
+        const size_t need = ((size_t)n64 * 8 + (size_t)n32 * 4) * nt + (size_t)m->n * 8;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess || need > fr / 4) {
+            cudaGetLastError();
+            if (nt > (1u << 22)) nt = 1u << 22;
+        }
+    }
     double *s64 = NULL, *vs = NULL;
     float *s32 = NULL;
     int rc = MB_OK;
