@@ -312,14 +312,39 @@ int mb_adjoint_forward(mb_adjoint *a, const double *sigma_cell, const double *sc
 int mb_adjoint_backward(mb_adjoint *a, const double *dtraces, double *grad_sigma, double *grad_scale_gkr);
 void mb_adjoint_destroy(mb_adjoint *a);
 
-/* Checkpoint / restore of the loop state (V, V*, the ODE state rows, the
- * clock and stimulus table, activation tracking) to host memory in this
- * library's own layout, for a tissue of the same shape, model and precision.
- * (The reference's save_simulation_state files, save_state.c:16-150, are not
- * read or written.)                                                          */
+/* Checkpoint / restore of the whole loop state (V, V*, the ODE state rows,
+ * the clock and stimulus table, activation tracking) to host memory in this
+ * library's own layout, for a tissue of the same shape, model and precision
+ * (the reference's layout: mb_monodomain_save_state below).                 */
 int mb_monodomain_checkpoint_bytes(mb_monodomain *m, size_t *bytes);
 int mb_monodomain_checkpoint(mb_monodomain *m, void *host, size_t bytes);
 int mb_monodomain_restore(mb_monodomain *m, const void *host, size_t bytes);
+/* Checkpoints in the reference's own layout: the three files of
+ * save_simulation_state (src/save_state_library/save_state.c:16-150) --
+ * grid_checkpoint.dat, monodomain_solver_checkpoint.dat and
+ * ode_solver_checkpoint.dat -- in the directory dir, which
+ * restore_simulation_state (restore_state.c:38-230) reads back into the
+ * reference's own loop, and which mb_monodomain_restore_state reads from the
+ * reference's.  The state vector is written in the reference's numbering of
+ * the active cells (the Hilbert order of its octree) and, with gpu_layout,
+ * state row after state row as its GPU build writes it (with the row pitch
+ * cudaMallocPitch gives on this device), else cell after cell as its CPU
+ * build does.  Restore checks the mesh, active cell count, dt, beta and cm
+ * against the tissue's and sets V, the ODE state and the loop clock (step
+ * count, time); activation tracking and the ECG records are not part of the
+ * layout.  Cell centres are matched exactly, as the reference matches them:
+ * spacings whose half-integer multiples are exact in double (100 um) are
+ * supported.                                                                 */
+int mb_monodomain_save_state(mb_monodomain *m, const char *dir, int gpu_layout);
+int mb_monodomain_restore_state(mb_monodomain *m, const char *dir);
+/* The reference's numbering of the active cells of an nx x ny x nz cuboid
+ * with an optional removed-cell mask (grid order, 0 = removed): order[r] =
+ * grid index of active cell r (order_grid_cells, grid.c:245-263, over the
+ * octree of set_cuboid_domain_mesh, domain_helpers.c:19-73); also the number
+ * of active cells and of all the octree's leaves.  Host only.  Any output
+ * may be NULL.                                                              */
+int mb_reference_cell_order(int nx, int ny, int nz, const uint8_t *active, int64_t *order, int64_t *n_active,
+                            int64_t *number_of_cells);
 /* V of the active cells in the format of save_as_text_or_binary
  * (save_mesh.c:248-420): "x,y,z,hx,hy,hz,V" per line, or 7 doubles per cell
  * when binary; cells in grid order.                                          */

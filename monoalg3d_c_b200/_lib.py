@@ -54,6 +54,7 @@ EXPORTED = [
     "mb_monodomain_device_v", "mb_monodomain_profile_steps", "mb_csr_conjugate_gradient",
     "mb_monodomain_tuning", "mb_monodomain_time_steps", "mb_monodomain_time_steps_host",
     "mb_csr_conjugate_gradient_noalloc", "mb_cg_launch_shapes",
+    "mb_monodomain_save_state", "mb_monodomain_restore_state", "mb_reference_cell_order",
 ]
 
 
@@ -177,6 +178,9 @@ def _load() -> C.CDLL:
         "mb_monodomain_time_steps": (i32, [vp, i32, P(dbl)]),
         "mb_monodomain_time_steps_host": (i32, [vp, i32, vp, vp, P(dbl)]),
         "mb_csr_conjugate_gradient_noalloc": (i32, [i32, vp, vp, vp, vp, vp, dbl, i32, i32, P(u32), P(dbl), vp]),
+        "mb_monodomain_save_state": (i32, [vp, C.c_char_p, i32]),
+        "mb_monodomain_restore_state": (i32, [vp, C.c_char_p]),
+        "mb_reference_cell_order": (i32, [i32, i32, i32, vp, vp, P(i64), P(i64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -253,6 +253,18 @@ class Tissue:
         buf = C.create_string_buffer(state, len(state))
         check(lib.mb_monodomain_restore(self._h, buf, len(state)))
 
+    def save_state(self, directory: str, gpu_layout: bool = False):
+        """The loop state in the three files of the reference's
+        save_simulation_state (grid, monodomain solver, ODE solver), which
+        the reference's restore_simulation_state reads back."""
+        check(lib.mb_monodomain_save_state(self._h, directory.encode(), 1 if gpu_layout else 0))
+
+    def restore_state(self, directory: str):
+        """V, the ODE state and the loop clock from the reference's
+        save_simulation_state files (written by the reference or by
+        save_state) for this tissue's mesh."""
+        check(lib.mb_monodomain_restore_state(self._h, directory.encode()))
+
     def save_v(self, path: str, binary: bool = False):
         """V of the active cells in the reference's save_as_text_or_binary format."""
         check(lib.mb_monodomain_save_v(self._h, path.encode(), 1 if binary else 0))
@@ -331,6 +343,17 @@ class Tissue:
         a, b, c, it = C.c_double(), C.c_double(), C.c_double(), C.c_int()
         check(lib.mb_monodomain_profile_steps(self._h, n, C.byref(a), C.byref(b), C.byref(c), C.byref(it)))
         return {"ode_ms": a.value, "cg_ms": b.value, "step_ms": c.value, "cg_iterations": it.value}
+
+
+def reference_cell_order(nx: int, ny: int, nz: int, active: Optional[np.ndarray] = None):
+    """The reference's numbering of a cuboid's active cells (grid indices in
+    its octree's Hilbert order) and the number of leaves of that octree."""
+    a = None if active is None else np.ascontiguousarray(active, dtype=np.uint8).reshape(-1)
+    n_act, n_leaves = C.c_int64(), C.c_int64()
+    check(lib.mb_reference_cell_order(nx, ny, nz, _ptr(a), None, C.byref(n_act), C.byref(n_leaves)))
+    order = np.empty(n_act.value, dtype=np.int64)
+    check(lib.mb_reference_cell_order(nx, ny, nz, _ptr(a), _ptr(order), C.byref(n_act), C.byref(n_leaves)))
+    return order, n_leaves.value
 
 
 def cg_launch_shapes() -> int:

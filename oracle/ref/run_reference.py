@@ -88,7 +88,9 @@ def ini_text(case: dict, work_dir: str, out_dir: str | None = None, dumps_every:
     celltype (None = every ToRORd cell ENDO, "x_45_25_30" = the stock
     transmural extra data, "z_thirds" = the adapter's); stims (list of
     dicts: kind "x_less_than" | "x_y_limits", start, duration, current,
-    x_limit | min, max); ecg (dict: leads, sigma_b, calc_rate) or None."""
+    x_limit | min, max); ecg (dict: leads, sigma_b, calc_rate) or None;
+    save_state (dict: output_dir, save_rate) and restore_state (dict:
+    input_dir) for the reference's checkpoint plugins, or None."""
     nx, ny, nz = case["nx"], case["ny"], case["nz"]
     dx = case.get("dx", 100.0)
     dt = case.get("dt", 0.02)
@@ -137,6 +139,15 @@ def ini_text(case: dict, work_dir: str, out_dir: str | None = None, dumps_every:
         # rate); the adapter writes the dumps every `dumps_every` steps
         save = (f"[save_result]\nprint_rate=1\noutput_dir={out_dir}\nmain_function=save_mb_v_every\n"
                 f"every={dumps_every}\nlibrary_file={LIBS}/libmb_adapters.so\n")
+    if case.get("save_state"):
+        # the plain checkpoint plugin (save_state.c:16-150); save_rate 0 = at
+        # the end of the run only
+        ss = case["save_state"]
+        save += (f"\n[save_state]\nsave_rate={int(ss.get('save_rate', 0))}\noutput_dir={ss['output_dir']}\n"
+                 f"main_function=save_simulation_state\nlibrary_file={LIBS}/libdefault_save_state.so\n")
+    if case.get("restore_state"):
+        save += (f"\n[restore_state]\ninput_dir={case['restore_state']['input_dir']}\n"
+                 f"main_function=restore_simulation_state\nlibrary_file={LIBS}/libdefault_restore_state.so\n")
     stims = case.get("stims") or [dict(kind="x_less_than", start=0.0, duration=2.0, current=-53.0, x_limit=500.0)]
     stim_text = "\n".join(_stim_section(i, s) for i, s in enumerate(stims))
     return f"""[main]
