@@ -69,7 +69,9 @@ extern "C" {
 /* ---- enumerations ------------------------------------------------------ */
 enum mb_model {
     MB_MODEL_TT2006 = 0,               /* libten_tusscher_2006, 19 states    */
-    MB_MODEL_TORORD_FKATP_MIXED = 1    /* libToRORd_fkatp_mixed_endo_mid_epi, 43 states */
+    MB_MODEL_TORORD_FKATP_MIXED = 1,   /* libToRORd_fkatp_mixed_endo_mid_epi, 43 states */
+    MB_MODEL_TORORD_FKATP_ENDO = 2     /* libToRORd_fkatp_endo, 43 states, forward Euler
+                                          (fixed or adaptive step, see ode_adaptive) */
 };
 
 enum mb_precision {
@@ -179,7 +181,24 @@ typedef struct mb_monodomain_desc {
     const double *ecg_leads;
     double ecg_sigma_b;                /* bath conductivity, sigma_b of the reference */
     int64_t ecg_capacity;
+    /* [ode_solver] adaptive = true, for the forward-Euler library
+       (MB_MODEL_TORORD_FKATP_ENDO; default_solvers.c:55-175): each cell
+       steps with its own error-controlled dt in [min_dt, max_dt], min_dt =
+       dt_ode (the reference takes 1e-10 when no dt is given,
+       ode_solver.c:311-328), max_dt = dt_pde, tolerances ode_abs_tol /
+       ode_rel_tol (default 1e-5).  Each
+       loop step integrates every cell up to cur_time + min_dt
+       (MB_ODE_ADAPTIVE_CPU, the CPU build's solve_model_odes_cpu) or up to
+       cur_time + max_dt (MB_ODE_ADAPTIVE_GPU, the GPU build's solve_gpu).   */
+    int    ode_adaptive;               /* enum mb_ode_adaptive                */
+    double ode_abs_tol, ode_rel_tol;
 } mb_monodomain_desc;
+
+enum mb_ode_adaptive {
+    MB_ODE_FIXED = 0,
+    MB_ODE_ADAPTIVE_CPU = 1,
+    MB_ODE_ADAPTIVE_GPU = 2
+};
 
 #define MB_ECG_MAX_LEADS 16
 
@@ -204,6 +223,12 @@ int mb_device_count(int *count);
 
 /* ---- cell model library (ode_solver.h:33-47) --------------------------- */
 int mb_init_cell_model_data(int model, int *number_of_ode_equations, double *initial_v);
+/* Initial state of the ToRORd_fkatp_endo library (43 values): its CPU
+ * build's (ToRORd_fkatp_endo.c:30-76, the default of a tissue) or, with
+ * gpu_build, its GPU build's, a different steady state
+ * (ToRORd_fkatp_endo.cu:8-50); pass the latter as initial_state to follow
+ * the GPU build.                                                            */
+int mb_torord_endo_initial_state(int gpu_build, double *state);
 
 /* Stand-alone ODE object: num_cells independent cells, state in SoA rows. */
 int mb_ode_create(mb_ode **out, int model, int precision, int rl_rule,

@@ -22,6 +22,10 @@ MB_ERR_STATE = 6
 
 MB_MODEL_TT2006 = 0
 MB_MODEL_TORORD_FKATP_MIXED = 1
+MB_MODEL_TORORD_FKATP_ENDO = 2
+MB_ODE_FIXED = 0
+MB_ODE_ADAPTIVE_CPU = 1
+MB_ODE_ADAPTIVE_GPU = 2
 MB_PREC_FP64 = 0
 MB_PREC_MIXED = 1
 MB_RL_REFERENCE_CPU = 0
@@ -55,6 +59,7 @@ EXPORTED = [
     "mb_monodomain_tuning", "mb_monodomain_time_steps", "mb_monodomain_time_steps_host",
     "mb_csr_conjugate_gradient_noalloc", "mb_cg_launch_shapes",
     "mb_monodomain_save_state", "mb_monodomain_restore_state", "mb_reference_cell_order",
+    "mb_torord_endo_initial_state",
 ]
 
 
@@ -102,6 +107,9 @@ class MbDesc(C.Structure):
         ("ecg_leads", C.c_void_p),
         ("ecg_sigma_b", C.c_double),
         ("ecg_capacity", C.c_int64),
+        ("ode_adaptive", C.c_int),
+        ("ode_abs_tol", C.c_double),
+        ("ode_rel_tol", C.c_double),
     ]
 
 
@@ -181,6 +189,7 @@ def _load() -> C.CDLL:
         "mb_monodomain_save_state": (i32, [vp, C.c_char_p, i32]),
         "mb_monodomain_restore_state": (i32, [vp, C.c_char_p]),
         "mb_reference_cell_order": (i32, [i32, i32, i32, vp, vp, P(i64), P(i64)]),
+        "mb_torord_endo_initial_state": (i32, [i32, P(dbl)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -37,6 +37,7 @@ void mb_fibre_tensor(const double f[3], const double s[3], const double n[3], do
 double mb_alpha(double beta, double cm, double dt, double dx, double dy, double dz);
 double mb_tt2006_default_state(int s);
 double mb_torord_default_state(int celltype, int s);
+double mb_torord_endo_default_state(int gpu_build, int s);
 int mb_monodomain_uses_graphs(mb_monodomain *m);
 
 #ifdef __cplusplus

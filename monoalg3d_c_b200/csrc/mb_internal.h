@@ -47,7 +47,7 @@ typedef struct mb_ctrl {
     int32_t refinements;
     int32_t use_precond;
     uint32_t ticket;
-    uint32_t pad_;
+    uint32_t ode_unfinished; /* cells whose adaptive ODE step ran out of passes */
     /* activation tracking (ODE kernels) */
     double  act_dt;          /* loop step dt_pde                            */
     float   act_threshold;   /* upward crossing that marks an activation    */
@@ -105,6 +105,12 @@ typedef struct mb_ode_dev {
     float  *out32;
     float  *act;              /* activation tracking, MB_ACT_ROWS rows of ld,
                                  NULL = off                                 */
+    /* adaptive forward Euler (MB_MODEL_TORORD_FKATP_ENDO): 0 = fixed step;
+       else sv64 rows NEQ..NEQ+2 hold each cell's dt, time_new, previous_dt
+       and a loop step integrates to cur_time + adapt_span                  */
+    int32_t adaptive;
+    double min_dt, max_dt, abs_tol, rel_tol, adapt_span;
+    double cur_time;          /* loop time when no control block is given   */
 } mb_ode_dev;
 
 /* Rows of the activation-tracking array (per compact cell). */

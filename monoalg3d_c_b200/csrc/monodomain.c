@@ -76,12 +76,27 @@ int mb_init_cell_model_data(int model, int *neq, double *initial_v) {
         if (initial_v) *initial_v = -88.763800;               /* ToRORd_fkatp_mixed_endo_mid_epi.h:11 */
         return MB_OK;
     }
+    if (model == MB_MODEL_TORORD_FKATP_ENDO) {
+        if (neq) *neq = MB_NEQ_TORORD;
+        if (initial_v) *initial_v = (double)-88.763800f;      /* ToRORd_fkatp_endo.h:5 */
+        return MB_OK;
+    }
     return set_err(MB_ERR_ARG, "unknown model %d", model);
 }
 
-/* Row counts of the SoA state for (model, precision). */
-static void ode_rows(int model, int precision, int *n64, int *n32) {
-    if (model == MB_MODEL_TT2006) {
+int mb_torord_endo_initial_state(int gpu_build, double *state) {
+    if (!state) return set_err(MB_ERR_ARG, "null state");
+    for (int s = 0; s < MB_NEQ_TORORD; ++s) state[s] = mb_torord_endo_default_state(gpu_build, s);
+    return MB_OK;
+}
+
+/* Row counts of the SoA state for (model, precision, adaptive ODE step). */
+static void ode_rows(int model, int precision, int adaptive, int *n64, int *n32) {
+    if (model == MB_MODEL_TORORD_FKATP_ENDO) {
+        /* FP64 in either precision; adaptive: + dt, time_new, previous_dt */
+        *n64 = MB_NEQ_TORORD + (adaptive ? 3 : 0);
+        *n32 = 0;
+    } else if (model == MB_MODEL_TT2006) {
         if (precision == MB_PREC_FP64) { *n64 = 19; *n32 = 0; }
         else { *n64 = 6; *n32 = 13; }
     } else {
@@ -112,14 +127,14 @@ int mb_ode_create(mb_ode **out, int model, int precision, int rl_rule, uint32_t 
     if (!o) return set_err(MB_ERR_NOMEM, "out of host memory");
     o->neq = neq;
     o->dev.model = model;
-    o->dev.precision = precision;
+    o->dev.precision = model == MB_MODEL_TORORD_FKATP_ENDO ? MB_PREC_FP64 : precision;
     o->dev.rl_rule = rl_rule;
     o->dev.num_steps = (int)num_steps;
     o->dev.n = num_cells;
     o->dev.ld = round_up32(num_cells);
     o->dev.dt = dt;
     int n64, n32;
-    ode_rows(model, precision, &n64, &n32);
+    ode_rows(model, precision, 0, &n64, &n32);
     cudaError_t e = cudaStreamCreateWithFlags(&o->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc((void **)&o->dev.sv64, (size_t)n64 * o->dev.ld * sizeof(double));
     if (e == cudaSuccess && n32) e = cudaMalloc((void **)&o->dev.sv32, (size_t)n32 * o->dev.ld * sizeof(float));
@@ -145,6 +160,10 @@ void mb_ode_destroy(mb_ode *o) {
 static int model_ic_table(int model, const double *initial_state, double *table, int *ntypes) {
     if (model == MB_MODEL_TT2006) {
         for (int s = 0; s < MB_NEQ_TT2006; ++s) table[s] = initial_state ? initial_state[s] : mb_tt2006_default_state(s);
+        *ntypes = 1;
+    } else if (model == MB_MODEL_TORORD_FKATP_ENDO) {
+        for (int s = 0; s < MB_NEQ_TORORD; ++s)
+            table[s] = initial_state ? initial_state[s] : mb_torord_endo_default_state(0, s);
         *ntypes = 1;
     } else {
         if (initial_state) {
@@ -188,9 +207,9 @@ int mb_set_model_initial_conditions_gpu(mb_ode *o, const double *initial_state, 
 }
 
 int mb_solve_model_odes_gpu(mb_ode *o, double current_t, const double *stim_currents) {
-    (void)current_t;
     if (!o) return set_err(MB_ERR_ARG, "null ode");
     mb_ode_dev dv = o->dev;
+    dv.cur_time = current_t;
     if (stim_currents) {
         CK(cudaMemcpyAsync(o->d_stim, stim_currents, (size_t)o->dev.n * sizeof(double), cudaMemcpyHostToDevice,
                            o->stream));
@@ -279,6 +298,9 @@ void mb_monodomain_desc_defaults(mb_monodomain_desc *d) {
     d->track_activation = 0;
     d->activation_threshold = -30.0;
     d->activation_min_interval = 10.0;
+    d->ode_adaptive = MB_ODE_FIXED;
+    d->ode_abs_tol = 1e-5;
+    d->ode_rel_tol = 1e-5;
 }
 
 /* alpha = ((beta * cm) / dt) * UM2_TO_CM2 * (dx dy dz), with UM2_TO_CM2 the
@@ -504,6 +526,16 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         return set_err(MB_ERR_ARG, "dx, dy, dz, dt_pde and dt_ode must be positive");
     if (d->num_stims < 0 || d->num_stims > MB_MAX_STIMS) return set_err(MB_ERR_ARG, "num_stims out of range");
     if (d->precision != MB_PREC_FP64 && d->precision != MB_PREC_MIXED) return set_err(MB_ERR_ARG, "bad precision");
+    if (d->ode_adaptive) {
+        if (d->model != MB_MODEL_TORORD_FKATP_ENDO)
+            return set_err(MB_ERR_ARG, "the adaptive ODE step belongs to the forward-Euler library (ToRORd_fkatp_endo)");
+        if (d->ode_adaptive != MB_ODE_ADAPTIVE_CPU && d->ode_adaptive != MB_ODE_ADAPTIVE_GPU)
+            return set_err(MB_ERR_ARG, "bad ode_adaptive");
+        if (!(d->ode_abs_tol > 0 && d->ode_rel_tol > 0 && d->dt_ode <= d->dt_pde))
+            return set_err(MB_ERR_ARG, "adaptive ODE step: tolerances must be positive and dt_ode <= dt_pde");
+    }
+    if (d->model == MB_MODEL_TORORD_FKATP_ENDO && (d->celltype || d->current_scale))
+        return set_err(MB_ERR_ARG, "ToRORd_fkatp_endo takes no cell types or conductance scalings");
     int neq;
     double model_v0;
     if (mb_init_cell_model_data(d->model, &neq, &model_v0)) return MB_ERR_ARG;
@@ -541,12 +573,22 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
 
     /* ODE state */
     int n64, n32;
-    ode_rows(d->model, d->precision, &n64, &n32);
+    ode_rows(d->model, d->precision, d->ode_adaptive, &n64, &n32);
     ALLOC(m->d_sv64, (size_t)n64 * ld * sizeof(double));
     if (n32) ALLOC(m->d_sv32, (size_t)n32 * ld * sizeof(float));
     m->ode.model = d->model;
-    m->ode.precision = d->precision;
+    m->ode.precision = d->model == MB_MODEL_TORORD_FKATP_ENDO ? MB_PREC_FP64 : d->precision;
     m->ode.rl_rule = d->rl_rule;
+    if (d->ode_adaptive) {
+        /* one adaptive pass per loop step (monodomain_solver.c:517-527) */
+        m->num_steps = 1;
+        m->ode.adaptive = d->ode_adaptive;
+        m->ode.min_dt = d->dt_ode > 0.0 ? d->dt_ode : 1e-10;
+        m->ode.max_dt = d->dt_pde;
+        m->ode.abs_tol = d->ode_abs_tol;
+        m->ode.rel_tol = d->ode_rel_tol;
+        m->ode.adapt_span = d->ode_adaptive == MB_ODE_ADAPTIVE_CPU ? m->ode.min_dt : m->ode.max_dt;
+    }
     m->ode.num_steps = m->num_steps;
     m->ode.n = na;
     m->ode.ld = ld;
@@ -612,6 +654,17 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
         cudaStreamSynchronize(m->stream);
         cudaFree(d_table);
         if (e) { rc = set_err(MB_ERR_CUDA, "ode init: %s", cudaGetErrorString((cudaError_t)e)); goto fail; }
+    }
+    if (m->ode.adaptive) {
+        /* per-cell dt = min_dt, time_new = previous_dt = 0
+         * (ToRORd_fkatp_endo.c:14-25) */
+        double *rows = (double *)calloc((size_t)3 * ld, sizeof(double));
+        if (!rows) { rc = set_err(MB_ERR_NOMEM, "host memory"); goto fail; }
+        for (uint32_t t = 0; t < ld; ++t) rows[t] = m->ode.min_dt;
+        cudaError_t e = cudaMemcpy(m->d_sv64 + (size_t)neq * ld, rows, (size_t)3 * ld * sizeof(double),
+                                   cudaMemcpyHostToDevice);
+        free(rows);
+        if (e != cudaSuccess) { rc = set_err(MB_ERR_CUDA, "adaptive rows: %s", cudaGetErrorString(e)); goto fail; }
     }
 
     /* V (grid): the CG initial guess is the assembly init value
@@ -914,7 +967,7 @@ static int ode_autotune(mb_monodomain *m) {
         return MB_OK;
     }
     int n64, n32;
-    ode_rows(m->desc.model, m->desc.precision, &n64, &n32);
+    ode_rows(m->desc.model, m->desc.precision, m->desc.ode_adaptive, &n64, &n32);
     /* every cell where the scratch outputs fit in a quarter of the free
      * device memory (launch shapes rank differently on a few waves of blocks
      * than on the hundreds of waves of a large tissue), else 4 M cells */
@@ -1150,6 +1203,13 @@ int mb_monodomain_sync(mb_monodomain *m) {
         if (st) return set_err(MB_ERR_CUDA, "CG grid barrier timed out (status %d)", st);
     }
     if (nan_flag) return set_err(MB_ERR_NAN, "NaN in the CG error: the cell model diverged");
+    if (m->ode.adaptive) {
+        uint32_t unfinished = 0;
+        CK(cudaMemcpy(&unfinished, &m->d_ctrl->ode_unfinished, sizeof unfinished, cudaMemcpyDeviceToHost));
+        if (unfinished)
+            return set_err(MB_ERR_NAN, "adaptive ODE step: %u cell steps did not reach the step's end time within "
+                                       "the pass limit", unfinished);
+    }
     return MB_OK;
 }
 
@@ -1600,7 +1660,7 @@ static size_t align256(size_t b) { return (b + 255u) & ~(size_t)255u; }
 /* snapshot layout: V | V* | FP64 state rows | FP32 state rows | control block */
 static void snapshot_layout(const mb_monodomain *m, size_t off[5], size_t len[5]) {
     int n64, n32;
-    ode_rows(m->desc.model, m->desc.precision, &n64, &n32);
+    ode_rows(m->desc.model, m->desc.precision, m->desc.ode_adaptive, &n64, &n32);
     len[0] = (size_t)m->n * sizeof(double);
     len[1] = (size_t)m->n * sizeof(double);
     len[2] = (size_t)n64 * m->ode.ld * sizeof(double);

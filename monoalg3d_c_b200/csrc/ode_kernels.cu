@@ -2,8 +2,58 @@
 // state gather/scatter.  The mixed-precision kernels live in ode_mixed.cu,
 // which is compiled with the fast FP32 math.
 #include "ode_common.cuh"
+#include "model_torord_endo.cuh"
 
 MB_NS_BEGIN
+
+// ---- ToRORd-fkatp endo, forward Euler (FP64 in either tissue precision) ----
+// Fixed step: num_steps Euler steps per loop step (default_solvers.c:37-53).
+// Adaptive: one error-controlled pass to cur_time + adapt_span, with the
+// cell's dt / time_new / previous_dt in sv64 rows NEQ..NEQ+2
+// (default_solvers.c:55-175); a cell that does not reach the end time within
+// the pass limit keeps its state and is counted in ctrl->ode_unfinished.
+constexpr int TORE_MAX_PASSES = 200000;
+
+template <int MINB, bool ADAPTIVE>
+__global__ void __launch_bounds__(ODE_THREADS, MINB)
+k_torord_endo(mb_ode_dev o, mb_ctrl *ctrl, const double *__restrict__ vin, double *__restrict__ vout) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= o.n) return;
+    const uint32_t g = o.cell ? o.cell[t] : t;
+    const double stim = cell_stim(o, ctrl, t);
+    const size_t ld = o.ld;
+    const double *src = (ctrl == nullptr || ctrl->cur_time > 0.0) ? vin : vout;
+    double y[mb_tore::NEQ];
+    y[0] = src[g];
+    act_track(o, ctrl, t, y[0]);
+#pragma unroll
+    for (int s = 1; s < mb_tore::NEQ; ++s) y[s] = o.sv64[s * ld + t];
+    double *w = out64(o);
+    const size_t wl = out_ld(o);
+    if (!ADAPTIVE) {
+        const double dt = o.dt;
+        for (int step = 0; step < o.num_steps; ++step) {
+            double d[mb_tore::NEQ];
+            mb_tore::rhs(y, stim, d);
+#pragma unroll
+            for (int s = 0; s < mb_tore::NEQ; ++s) y[s] = dt * d[s] + y[s];
+        }
+    } else {
+        double h = o.sv64[(size_t)mb_tore::NEQ * ld + t];
+        double tn = o.sv64[(size_t)(mb_tore::NEQ + 1) * ld + t];
+        double pdt = o.sv64[(size_t)(mb_tore::NEQ + 2) * ld + t];
+        const double now = ctrl ? ctrl->cur_time : o.cur_time;
+        const mb_tore::Adaptive p{o.min_dt, o.max_dt, o.abs_tol, o.rel_tol, TORE_MAX_PASSES};
+        if (!mb_tore::adaptive_step(y, stim, now + o.adapt_span, p, h, tn, pdt) && ctrl)
+            atomicAdd(&ctrl->ode_unfinished, 1u);
+        w[(size_t)mb_tore::NEQ * wl + t] = h;
+        w[(size_t)(mb_tore::NEQ + 1) * wl + t] = tn;
+        w[(size_t)(mb_tore::NEQ + 2) * wl + t] = pdt;
+    }
+    vout[g] = y[0];
+#pragma unroll
+    for (int s = 1; s < mb_tore::NEQ; ++s) w[s * wl + t] = y[s];
+}
 
 // Row of state s in the (precision, model) layout: returns row and whether it
 // is a double row.
@@ -84,9 +134,25 @@ extern "C" int mbk_ode_init(const mb_ode_dev *o, const double *table_dev, int nt
 
 extern "C" int mbk_ode_step(const mb_ode_dev *o, mb_ctrl *ctrl, const double *vin, double *vout, cudaStream_t s) {
     if (o->n == 0) return 0;
-    if (o->precision != MB_PREC_FP64) return mbk_ode_step_mixed(o, ctrl, vin, vout, s);
     const unsigned blocks = (o->n + ODE_THREADS - 1) / ODE_THREADS;
     const mb_ode_dev &a = *o;
+    if (o->model == MB_MODEL_TORORD_FKATP_ENDO) {
+        // one-launch kernels only (the staged variants fall back to them)
+#define L(MB, AD) k_torord_endo<MB, AD><<<blocks, ODE_THREADS, 0, s>>>(a, ctrl, vin, vout)
+        if (o->adaptive) {
+            L(1, true);
+        } else {
+            switch (o->variant) {
+            case 0: L(1, false); break;
+            case 1: L(2, false); break;
+            case 2: L(3, false); break;
+            default: L(4, false); break;
+            }
+        }
+#undef L
+        return (int)cudaGetLastError();
+    }
+    if (o->precision != MB_PREC_FP64) return mbk_ode_step_mixed(o, ctrl, vin, vout, s);
 #define MB_STAGED(KERNEL, N64, N32)                                                       \
     do {                                                                                  \
         const size_t sm = staged_smem(N64, N32);                                          \
@@ -132,3 +198,6 @@ extern "C" int mbk_ode_scatter(const mb_ode_dev *o, const double *in_dev, double
 
 extern "C" double mb_tt2006_default_state(int s) { return tt2006_default_state(s); }
 extern "C" double mb_torord_default_state(int celltype, int s) { return torord_default_state(celltype, s); }
+extern "C" double mb_torord_endo_default_state(int gpu_build, int s) {
+    return gpu_build ? mb_tore::initial_state_gpu(s) : mb_tore::initial_state_cpu(s);
+}

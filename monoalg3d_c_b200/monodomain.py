@@ -24,7 +24,9 @@ from ._lib import MbDesc, MbStepStats, MbStim, check, lib
 
 MODELS = {"tt2006": _lib.MB_MODEL_TT2006, "ten_tusscher_2006": _lib.MB_MODEL_TT2006,
           "torord": _lib.MB_MODEL_TORORD_FKATP_MIXED,
-          "ToRORd_fkatp_mixed_endo_mid_epi": _lib.MB_MODEL_TORORD_FKATP_MIXED}
+          "ToRORd_fkatp_mixed_endo_mid_epi": _lib.MB_MODEL_TORORD_FKATP_MIXED,
+          "torord_endo": _lib.MB_MODEL_TORORD_FKATP_ENDO, "ToRORd_fkatp_endo": _lib.MB_MODEL_TORORD_FKATP_ENDO}
+ODE_ADAPTIVE = {None: _lib.MB_ODE_FIXED, "cpu": _lib.MB_ODE_ADAPTIVE_CPU, "gpu": _lib.MB_ODE_ADAPTIVE_GPU}
 PRECISIONS = {"fp64": _lib.MB_PREC_FP64, "mixed": _lib.MB_PREC_MIXED}
 RL_RULES = {"reference_cpu": _lib.MB_RL_REFERENCE_CPU, "true": _lib.MB_RL_TRUE}
 ASSEMBLIES = {"homogeneous": _lib.MB_ASSEMBLY_HOMOGENEOUS, "anisotropic": _lib.MB_ASSEMBLY_ANISOTROPIC,
@@ -42,6 +44,14 @@ def init_cell_model_data(model: str):
     neq, v0 = C.c_int(), C.c_double()
     check(lib.mb_init_cell_model_data(MODELS[model], C.byref(neq), C.byref(v0)))
     return neq.value, v0.value
+
+
+def torord_endo_initial_state(gpu_build: bool = False) -> np.ndarray:
+    """The ToRORd_fkatp_endo library's initial state: its CPU build's (the
+    tissue default) or its GPU build's (pass as initial_state to follow it)."""
+    out = np.empty(43, dtype=np.float64)
+    check(lib.mb_torord_endo_initial_state(1 if gpu_build else 0, out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out
 
 
 def loop_steps(final_time: float, dt: float) -> int:
@@ -82,10 +92,14 @@ def build_desc(nx: int, ny: int, nz: int, dx: float = 100.0, dy: float = 100.0, 
                stims: Sequence[Stim] = (), initial_v: float = float("nan"), track_activation: bool = False,
                activation_threshold: float = -30.0, activation_min_interval: float = 10.0,
                ecg_leads: Optional[Sequence[Sequence[float]]] = None, ecg_rate: int = 1, ecg_sigma_b: float = 1.0,
-               ecg_capacity: int = 100000) -> Tuple[MbDesc, list]:
+               ecg_capacity: int = 100000, ode_adaptive: Optional[str] = None, ode_abs_tol: float = 1e-5,
+               ode_rel_tol: float = 1e-5) -> Tuple[MbDesc, list]:
     """The C-ABI tissue description (mb_monodomain_desc) for these arguments,
     with the arrays it points to (keep them alive while the description is
-    in use).  Arrays given per cell are in grid order."""
+    in use).  Arrays given per cell are in grid order.  ode_adaptive ("cpu"
+    or "gpu", forward-Euler model only) selects the adaptive ODE step with
+    the reference CPU or GPU build's step end; its min_dt is dt_ode (1e-10
+    when dt_ode is None, as the reference with no dt), max_dt is dt_pde."""
     n = nx * ny * nz
     d = MbDesc()
     lib.mb_monodomain_desc_defaults(C.byref(d))
@@ -104,7 +118,9 @@ def build_desc(nx: int, ny: int, nz: int, dx: float = 100.0, dy: float = 100.0, 
 
     d.active = arr(active, np.uint8, n)
     d.dt_pde = dt_pde
-    d.dt_ode = dt_pde if dt_ode is None else dt_ode
+    d.dt_ode = (1e-10 if ode_adaptive else dt_pde) if dt_ode is None else dt_ode
+    d.ode_adaptive = ODE_ADAPTIVE[ode_adaptive]
+    d.ode_abs_tol, d.ode_rel_tol = ode_abs_tol, ode_rel_tol
     d.beta, d.cm = beta, cm
     d.model = MODELS[model]
     d.precision = PRECISIONS[precision]
@@ -167,7 +183,8 @@ class Tissue:
                  stims: Sequence[Stim] = (), initial_v: float = float("nan"), track_activation: bool = False,
                  activation_threshold: float = -30.0, activation_min_interval: float = 10.0,
                  ecg_leads: Optional[Sequence[Sequence[float]]] = None, ecg_rate: int = 1, ecg_sigma_b: float = 1.0,
-                 ecg_capacity: int = 100000):
+                 ecg_capacity: int = 100000, ode_adaptive: Optional[str] = None, ode_abs_tol: float = 1e-5,
+                 ode_rel_tol: float = 1e-5):
         self.shape = (nz, ny, nx)
         self.n = nx * ny * nz
         d, keep = build_desc(nx, ny, nz, dx, dy, dz, active=active, dt_pde=dt_pde, dt_ode=dt_ode, beta=beta,
@@ -179,7 +196,8 @@ class Tissue:
                              use_preconditioner=use_preconditioner, stims=stims, initial_v=initial_v,
                              track_activation=track_activation, activation_threshold=activation_threshold,
                              activation_min_interval=activation_min_interval, ecg_leads=ecg_leads,
-                             ecg_rate=ecg_rate, ecg_sigma_b=ecg_sigma_b, ecg_capacity=ecg_capacity)
+                             ecg_rate=ecg_rate, ecg_sigma_b=ecg_sigma_b, ecg_capacity=ecg_capacity,
+                             ode_adaptive=ode_adaptive, ode_abs_tol=ode_abs_tol, ode_rel_tol=ode_rel_tol)
         self.model = model
         self.precision = precision
         self._n_leads = 0 if ecg_leads is None else int(np.asarray(ecg_leads).reshape(-1, 3).shape[0])

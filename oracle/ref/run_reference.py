@@ -27,7 +27,8 @@ REF = os.path.join(os.path.dirname(HERE), "_ref")
 BIN = os.path.join(REF, "bin", "MonoAlg3D")
 LIBS = os.path.join(REF, "shared_libs")
 
-MODEL_LIBS = {"tt2006": "libten_tusscher_2006.so", "torord": "libToRORd_fkatp_mixed_endo_mid_epi.so"}
+MODEL_LIBS = {"tt2006": "libten_tusscher_2006.so", "torord": "libToRORd_fkatp_mixed_endo_mid_epi.so",
+              "torord_endo": "libToRORd_fkatp_endo.so"}
 
 
 def available() -> bool:
@@ -90,7 +91,9 @@ def ini_text(case: dict, work_dir: str, out_dir: str | None = None, dumps_every:
     dicts: kind "x_less_than" | "x_y_limits", start, duration, current,
     x_limit | min, max); ecg (dict: leads, sigma_b, calc_rate) or None;
     save_state (dict: output_dir, save_rate) and restore_state (dict:
-    input_dir) for the reference's checkpoint plugins, or None."""
+    input_dir) for the reference's checkpoint plugins, or None; dt_ode (ms,
+    default dt); adaptive (bool, forward-Euler model "torord_endo") with
+    abs_tol, rel_tol."""
     nx, ny, nz = case["nx"], case["ny"], case["nz"]
     dx = case.get("dx", 100.0)
     dt = case.get("dt", 0.02)
@@ -148,6 +151,14 @@ def ini_text(case: dict, work_dir: str, out_dir: str | None = None, dumps_every:
     if case.get("restore_state"):
         save += (f"\n[restore_state]\ninput_dir={case['restore_state']['input_dir']}\n"
                  f"main_function=restore_simulation_state\nlibrary_file={LIBS}/libdefault_restore_state.so\n")
+    # ODE step: dt_ode (default dt); adaptive forward Euler with "adaptive"
+    # (dt_ode None there = no dt line: the reference's min_dt of 1e-10)
+    ode_dt = case.get("dt_ode", None if case.get("adaptive") else dt)
+    ode_dt = "" if ode_dt is None else f"dt={ode_dt!r}\n"
+    ode_adaptive = ""
+    if case.get("adaptive"):
+        ode_adaptive = (f"adaptive=true\nabstol={case.get('abs_tol', 1e-5)!r}\n"
+                        f"reltol={case.get('rel_tol', 1e-5)!r}\n")
     stims = case.get("stims") or [dict(kind="x_less_than", start=0.0, duration=2.0, current=-53.0, x_limit=500.0)]
     stim_text = "\n".join(_stim_section(i, s) for i, s in enumerate(stims))
     return f"""[main]
@@ -188,8 +199,7 @@ side_length_z={nz * dx}
 library_file={LIBS}/{domain_lib}
 
 [ode_solver]
-dt={dt}
-use_gpu=no
+{ode_dt}{ode_adaptive}use_gpu=no
 gpu_id=0
 library_file={LIBS}/{MODEL_LIBS[case['model']]}
 

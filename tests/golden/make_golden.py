@@ -10,8 +10,11 @@ the centres) and keeps V at those steps, the CG iterations and error of every
 step from the solver log and, for the ECG case, the reference's ecg.txt.
 Inputs the stock plugins cannot express (removed-cell masks, fibres rotating
 through the thickness, z-layered ToRORd cell types) go through the adapter
-plugins of oracle/ref/adapters.c.  Runs only where the reference tree was
-built; the fixtures are committed and the tests read only them.
+plugins of oracle/ref/adapters.c.  torord_endo_steps holds one
+forward-Euler step of the ToRORd_fkatp_endo library from many states (its
+own solve_model_ode_cpu, called from the built plugin) and its CPU initial
+state.  Runs only where the reference tree was built; the fixtures are
+committed and the tests read only them.
 """
 from __future__ import annotations
 
@@ -64,13 +67,26 @@ CASES = {
     "torord_rotating_transmural": dict(nx=32, ny=16, nz=6, model="torord", assembly="anisotropic",
                                        fibre_rotate=(60.0, -60.0), sigma_l=0.0002, sigma_t=0.00004,
                                        z_thirds=True, sim_ms=12.0),
+    # the forward-Euler library ToRORd_fkatp_endo, fixed step: dt_pde = dt_ode
+    # = 2 us (its Euler step needs dt below twice the 1 us floor of the
+    # release time constant; with num_steps > 1 the reference also sums the
+    # stimulus of every sub-step into each of them)
+    "torord_fkatp_endo_euler": dict(nx=32, ny=16, nz=3, model="torord_endo", assembly="homogeneous", dt=0.002,
+                                    sim_ms=6.0, print_rate=500),
+    # the same library with the adaptive Euler step as the stock examples run
+    # it (adaptive = true, no ODE dt: min_dt 1e-10, max_dt = dt_pde)
+    "torord_fkatp_endo_adaptive": dict(nx=32, ny=16, nz=3, model="torord_endo", assembly="homogeneous",
+                                       adaptive=True, sim_ms=12.0),
 }
 
 
 def reference_case(case: dict) -> dict:
     """The run_reference case of a fixture case."""
-    c = dict(nx=case["nx"], ny=case["ny"], nz=case["nz"], dx=DX, dt=DT, model=case["model"],
+    c = dict(nx=case["nx"], ny=case["ny"], nz=case["nz"], dx=DX, dt=case.get("dt", DT), model=case["model"],
              assembly=case["assembly"], sim_ms=case["sim_ms"])
+    for k in ("dt_ode", "adaptive"):
+        if k in case:
+            c[k] = case[k]
     if case["assembly"] == "homogeneous":
         c["sigma"] = (0.00013, 0.00013, 0.00013)
     else:
@@ -92,19 +108,70 @@ def reference_case(case: dict) -> dict:
 
 
 def run_case(name: str, case: dict) -> dict:
-    r = rr.run_case(reference_case(case), threads=4, dumps_every=PRINT_RATE)
+    every = case.get("print_rate", PRINT_RATE)
+    r = rr.run_case(reference_case(case), threads=4, dumps_every=every)
     res = dict(V=r["V"], counts=r["counts"], its=r["its"], errors=r["errors"],
-               config=json.dumps(dict(case, dx=DX, dt=DT, print_rate=PRINT_RATE)))
+               config=json.dumps(dict(case, dx=DX, dt=case.get("dt", DT), print_rate=every)))
     if case.get("ecg"):
         res["ecg_t"] = r["ecg_t"]
         res["ecg"] = r["ecg"]
     return res
 
 
+def torord_endo_steps(n: int = 1024, dt: float = 0.002, seed: int = 11) -> dict:
+    """One forward-Euler step of the ToRORd_fkatp_endo library
+    (solve_model_ode_cpu, default_solvers.c:42-53) from n states: the
+    library's CPU initial state with every state perturbed by up to +-5 %,
+    V swept from -90 to +40 mV, every third cell stimulated (-53)."""
+    import ctypes as C
+    lib = C.CDLL(os.path.join(rr.LIBS, "libToRORd_fkatp_endo.so"))
+    lib.solve_model_ode_cpu.argtypes = [C.c_double, C.POINTER(C.c_double), C.c_double]
+    lib.set_model_initial_conditions_cpu.restype = None
+    rng = np.random.Generator(np.random.Philox(seed))
+    y0 = np.empty((n, 43))
+    base = _endo_cpu_initial_state(lib)
+    y0[:] = base * (1.0 + rng.uniform(-0.05, 0.05, size=(n, 43)))
+    y0[:, 0] = np.linspace(-90.0, 40.0, n)
+    stim = np.where(np.arange(n) % 3 == 0, -53.0, 0.0)
+    y1 = y0.copy()
+    for i in range(n):
+        row = np.ascontiguousarray(y1[i])
+        lib.solve_model_ode_cpu(dt, row.ctypes.data_as(C.POINTER(C.c_double)), stim[i])
+        y1[i] = row
+    return dict(y0=y0, y1=y1, stim=stim, dt=np.float64(dt), initial_state=base)
+
+
+def _endo_cpu_initial_state(lib) -> np.ndarray:
+    """The library's own CPU initial state: set_model_initial_conditions_cpu
+    (ToRORd_fkatp_endo.c:4-78) on a one-cell struct ode_solver, of which the
+    call reads original_num_cells and adaptive and sets sv (the leading
+    members of ode_solver.h:49-70, mirrored up to sv, then padding)."""
+    import ctypes as C
+
+    class OdeSolverHead(C.Structure):
+        _fields_ = [("handle", C.c_void_p), ("max_dt", C.c_double), ("min_dt", C.c_double),
+                    ("auto_dt", C.c_bool), ("adaptive", C.c_bool), ("rel_tol", C.c_double),
+                    ("abs_tol", C.c_double), ("num_cells_to_solve", C.c_size_t),
+                    ("cells_to_solve", C.c_void_p), ("num_steps", C.c_uint32), ("gpu", C.c_bool),
+                    ("gpu_id", C.c_int), ("original_num_cells", C.c_uint32),
+                    ("sv", C.POINTER(C.c_double)), ("rest", C.c_char * 1024)]
+
+    solver = OdeSolverHead()
+    solver.original_num_cells = 1
+    solver.adaptive = False
+    lib.set_model_initial_conditions_cpu.argtypes = [C.POINTER(OdeSolverHead), C.c_void_p]
+    lib.set_model_initial_conditions_cpu(C.byref(solver), None)
+    return np.array([solver.sv[i] for i in range(43)])
+
+
 def main(names=None, out_dir=HERE):
     if not rr.available():
         sys.exit(f"{rr.BIN} and the adapter plugins are not built: run `make -C oracle/ref` first")
-    for name in names or CASES:
+    for name in names or list(CASES) + ["torord_endo_steps"]:
+        if name == "torord_endo_steps":
+            np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **torord_endo_steps())
+            print(f"{name}: one Euler step of the endo library from 1024 states")
+            continue
         res = run_case(name, CASES[name])
         np.savez_compressed(os.path.join(out_dir, f"{name}.npz"), **res)
         print(f"{name}: {len(res['its'])} steps, {len(res['counts'])} dumps, mean CG its {res['its'].mean():.2f}")

@@ -9,6 +9,8 @@ import numpy as np
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASE_NAMES = ["tt2006_cuboid", "torord_endo_cuboid", "torord_transmural_cuboid", "tt2006_aniso_x",
               "tt2006_aniso_30", "torord_fibrosis_aniso", "torord_rotating_transmural"]
+# the forward-Euler library (ToRORd_fkatp_endo): fixed and adaptive step
+ENDO_CASE_NAMES = ["torord_fkatp_endo_euler", "torord_fkatp_endo_adaptive"]
 SEED_MASK = 1001
 
 
@@ -52,6 +54,10 @@ def tissue_kwargs(cfg: dict) -> dict:
                         >= cfg["fibrosis"]).astype(np.uint8)
     if cfg.get("extra_data"):
         kw["celltype"] = transmural_celltype(nx, ny, nz, cfg["dx"])
+    if cfg.get("dt_ode"):
+        kw["dt_ode"] = cfg["dt_ode"]
+    if cfg.get("adaptive"):
+        kw["ode_adaptive"] = "cpu"     # the reference CPU build's adaptive Euler
     if cfg.get("z_thirds"):
         ct = np.minimum(2, (3 * np.arange(nz)) // nz).astype(np.uint8)
         kw["celltype"] = np.broadcast_to(ct[:, None, None], (nz, ny, nx)).reshape(-1).copy()

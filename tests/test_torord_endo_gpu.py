@@ -1,0 +1,115 @@
+"""The forward-Euler library ToRORd_fkatp_endo on the GPU against the
+reference's own build of it (fixtures from tests/golden/make_golden.py):
+
+  - one Euler step from 1024 perturbed states (the library's
+    solve_model_ode_cpu), through the standalone cell-model API: within
+    1e-12 relative (the right-hand side is restated term for term, with the
+    library's single-precision parameters; only the exp / log / pow of the
+    two math libraries differ);
+  - a tissue with the fixed step (dt 2 us, 3000 loop steps): the FP64 bar,
+    V within 1e-8 relative + 1e-9 mV at every dump, CG iterations per step
+    equal (a step may differ by one);
+  - a tissue with the adaptive step as the stock examples run it (no ODE dt:
+    min_dt 1e-10, max_dt = dt_pde, tolerances 1e-5): V within 1e-6
+    relative + 1e-6 mV.  Each cell's step size follows its error estimate;
+    a last-bit difference in that estimate moves the step sizes by as much
+    and the solution by a fraction of the 1e-5 tolerance, so the bar is the
+    tolerance's scale, not the fixed step's."""
+import numpy as np
+import pytest
+
+import golden_cases as gc
+
+pytestmark = pytest.mark.gpu
+
+
+def test_single_step_matches_the_library():
+    from monoalg3d_c_b200.monodomain import OdeSolver
+    z = np.load(f"{gc.GOLDEN}/torord_endo_steps.npz")
+    y0, y1, stim, dt = z["y0"], z["y1"], z["stim"], float(z["dt"])
+    n = y0.shape[0]
+    o = OdeSolver("torord_endo", n, dt, 1)
+    o.set_model_initial_conditions_gpu()
+    o.set_state(y0.T)
+    o.solve_model_odes_gpu(0.0, stim)
+    got = o.state().T
+    o.close()
+    assert np.array_equal(np.isnan(got), np.isnan(y1))
+    ok = np.isfinite(y1)
+    err = np.abs(got[ok] - y1[ok])
+    assert np.all(err <= 1e-12 * np.abs(y1[ok]) + 1e-300), f"max rel {np.max(err / (np.abs(y1[ok]) + 1e-300)):.3e}"
+
+
+def _run(name, **over):
+    from monoalg3d_c_b200 import Tissue
+    g = gc.load(name)
+    cfg = g["config"]
+    kw = gc.tissue_kwargs(cfg)
+    kw.update(over)
+    t = Tissue(cfg["nx"], cfg["ny"], cfg["nz"], **kw)
+    out, done = {}, 0
+    for c in g["counts"]:
+        t.step(int(c) - done)
+        done = int(c)
+        out[int(c)] = t.v()
+    nsteps = len(g["its"])
+    t.step(nsteps - done)
+    stats = t.step_stats(0, nsteps)
+    t.sync()
+    t.close()
+    return g, out, stats
+
+
+def _check(name, g, out, rel, ab):
+    worst = 0.0
+    for q, c in enumerate(g["counts"]):
+        ref = g["V"][q]
+        err = np.abs(out[int(c)] - ref)
+        worst = max(worst, float(err.max()))
+        assert np.all(err <= rel * np.abs(ref) + ab), f"{name} step {c}: max |dV| {err.max():.3e} mV"
+    return worst
+
+
+def test_fixed_step_tissue_matches_reference():
+    name = "torord_fkatp_endo_euler"
+    g, out, stats = _run(name)
+    _check(name, g, out, 1e-8, 1e-9)
+    d_its = np.abs(stats["its"] - g["its"])
+    assert (d_its <= 1).all() and (d_its > 0).mean() < 0.02, f"CG iteration counts differ: {d_its.sum()}"
+
+
+def test_adaptive_step_tissue_matches_reference():
+    name = "torord_fkatp_endo_adaptive"
+    g, out, stats = _run(name)
+    worst = _check(name, g, out, 1e-6, 1e-6)
+    print(f"{name}: max |dV| {worst:.3e} mV")
+
+
+def test_mixed_tissue_runs_the_fp64_cell_model():
+    """The library has no mixed-precision form: a mixed tissue steps it in
+    FP64 and only the CG is mixed, within the mixed bar of the FP64 run."""
+    name = "torord_fkatp_endo_euler"
+    g, out, _ = _run(name, precision="mixed")
+    c = int(g["counts"][-1])
+    dv = out[c] - g["V"][-1]
+    assert float(np.sqrt(np.mean(dv ** 2))) <= 0.5
+
+
+def test_adaptive_gpu_rule_integrates_a_step_ahead():
+    """The GPU build's adaptive rule integrates each loop step to cur_time +
+    max_dt (one step ahead of the CPU build's cur_time + min_dt); both
+    complete every cell step."""
+    from monoalg3d_c_b200 import Tissue
+    g = gc.load("torord_fkatp_endo_adaptive")
+    kw = gc.tissue_kwargs(g["config"])
+    cfg = g["config"]
+    vs = []
+    for rule in ("cpu", "gpu"):
+        kw["ode_adaptive"] = rule
+        t = Tissue(cfg["nx"], cfg["ny"], cfg["nz"], **kw)
+        t.step(100)
+        t.sync()
+        vs.append(t.v())
+        t.close()
+    assert np.isfinite(vs[0]).all() and np.isfinite(vs[1]).all()
+    assert not np.array_equal(vs[0], vs[1])
