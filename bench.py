@@ -1,7 +1,7 @@
 """Benchmark of the operator-split monodomain step (cell-steps/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--repeats R] [--config 4]
-                    [--impl ours|reference]
+                    [--impl ours|reference|reference-gpu]
 
 A step is one iteration of the reference time loop (ODE sub-steps,
 update_monodomain, Jacobi-PCG to r.r <= 1e-16, clock) on the whole tissue.
@@ -25,7 +25,11 @@ e2e    -- the same steps through the reference-host C-ABI call with host
 the host's cores) on the same tissue -- adapter plugins express the
 removed-cell mask, the rotating fibres and the z-layered cell types -- over a
 bounded number of loop steps, by its own clocks; that process maps none of
-this repository's CUDA code.
+this repository's CUDA code.  --impl reference-gpu times the reference's own
+GPU build (oracle/_ref/cuda: its host loop, its GPU cell-model kernels and
+its FP32 cuSPARSE/cuBLAS conjugate gradient) the same way, with the settings
+of its GPU examples (no preconditioner, tolerance 1e-16, at most 200
+iterations) -- the existing GPU code on the same GPU and tissue.
 Under torchrun each rank runs an independent replica (the path does not shard:
 one GPU solves one tissue), so scaling is weak.
 """
@@ -58,7 +62,7 @@ def parse():
     ap.add_argument("--repeats", type=int, default=5)
     ap.add_argument("--config", type=int, default=4, choices=[0, 1, 2, 4])
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--ref-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the untimed activation-time comparison")
@@ -368,6 +372,29 @@ def reference_arm(args, wl, metric):
         "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def reference_gpu_arm(args, wl, metric):
+    """--impl reference-gpu: the reference's GPU build on the same tissue."""
+    rr, case = reference_case(wl)
+    if not rr.cuda_available():
+        print(json.dumps({"impl": "reference_gpu", "unavailable": "the reference's GPU build (oracle/_ref/cuda) "
+                                                                  "is not present"}))
+        return
+    gcase = dict(case, use_gpu=True, preconditioner=False)
+    r = reference_sample(rr, gcase, max(args.ref_steps, 3))
+    v = r["cell_steps_per_s"]
+    print(json.dumps({
+        "impl": "reference_gpu", "metric": metric, "value": v, "unit": "cell-steps/s", "n_gpus": 1,
+        "steps": r["steps"], "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True,
+        "dtype": "f64 cell model, f32 CG", "data": "synthetic",
+        "config": {"workload": wl.name, "cells": wl.n, "active_cells": wl.active_cells(),
+                   "sampled_cells": int(r["cells"]), "same_tissue": bool(r["whole_tissue"])},
+        "settings": "reference GPU build (oracle/_ref/cuda, kernels for sm_100a): GPU cell model, FP32 "
+                    "cuSPARSE/cuBLAS CG without preconditioner, tolerance 1e-16 on r.r, at most 200 iterations "
+                    "(its GPU examples' settings); its own clocks, Resolution Time - Total Write Time",
+        "phases_s": {"ode": r["ode_s"], "cg": r["cg_s"]},
+        "cg_iterations_per_step": r["cg_iterations"] / r["steps"]}))
+
+
 def main():
     args = parse()
     # at least 3 untimed warm-up steps, whatever was asked; the line reports
@@ -377,6 +404,10 @@ def main():
     metric = "cell-steps/s (mixed precision)"
     # the workload descriptions load none of the product's native code
     from monoalg3d_c_b200 import workloads
+    if args.impl == "reference-gpu":
+        if int(os.environ.get("RANK", "0")) == 0:
+            reference_gpu_arm(args, workloads.CONFIGS[args.config](args.scale), metric)
+        return
     if args.impl == "reference":
         # rank 0 alone runs the reference; no process group is needed
         if int(os.environ.get("RANK", "0")) == 0:

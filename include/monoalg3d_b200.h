@@ -229,6 +229,11 @@ int mb_init_cell_model_data(int model, int *number_of_ode_equations, double *ini
  * (ToRORd_fkatp_endo.cu:8-50); pass the latter as initial_state to follow
  * the GPU build.                                                            */
 int mb_torord_endo_initial_state(int gpu_build, double *state);
+/* Default initial state of the ToRORd_fkatp_mixed_endo_mid_epi library for
+ * a cell type (0 endo, 1 mid, 2 epi; 43 values): the steady states it and
+ * the ToRORd extra data tabulate (ToRORd_fkatp_mixed_endo_mid_epi.c:110-154,
+ * helper_functions.c:166-300).                                              */
+int mb_torord_initial_state(int celltype, double *state);
 
 /* Stand-alone ODE object: num_cells independent cells, state in SoA rows. */
 int mb_ode_create(mb_ode **out, int model, int precision, int rl_rule,
@@ -251,6 +256,15 @@ int mb_ode_set_state(mb_ode *ode, const double *host_state);
  * monodomain_solver.c:1051, update_monodomain.c:50).                       */
 int mb_ode_set_v(mb_ode *ode, const double *v, size_t stride);
 int mb_ode_get_v(mb_ode *ode, double *v, size_t stride);
+/* The device state itself: *sv = row 0 of the FP64 state rows (V, then the
+ * other states, one row of num_cells values every *pitch bytes), the pitched
+ * array the reference's GPU build keeps in ode_solver->sv and reads and
+ * writes row 0 of (update_ode_state_vector, monodomain_solver.c:1026-1045;
+ * update_monodomain.c:31-52).  FP64 objects only.                          */
+int mb_ode_device_state(mb_ode *ode, double **sv, size_t *pitch);
+/* Changes the sub-step size and count of later solves (the reference sets
+ * num_steps after the initial conditions, monodomain_solver.c:512-520).    */
+int mb_ode_set_steps(mb_ode *ode, double dt, uint32_t num_steps);
 void mb_ode_destroy(mb_ode *ode);
 
 /* ---- monodomain tissue ------------------------------------------------- */

@@ -59,7 +59,7 @@ EXPORTED = [
     "mb_monodomain_tuning", "mb_monodomain_time_steps", "mb_monodomain_time_steps_host",
     "mb_csr_conjugate_gradient_noalloc", "mb_cg_launch_shapes",
     "mb_monodomain_save_state", "mb_monodomain_restore_state", "mb_reference_cell_order",
-    "mb_torord_endo_initial_state",
+    "mb_torord_endo_initial_state", "mb_torord_initial_state", "mb_ode_device_state", "mb_ode_set_steps",
 ]
 
 
@@ -190,6 +190,9 @@ def _load() -> C.CDLL:
         "mb_monodomain_restore_state": (i32, [vp, C.c_char_p]),
         "mb_reference_cell_order": (i32, [i32, i32, i32, vp, vp, P(i64), P(i64)]),
         "mb_torord_endo_initial_state": (i32, [i32, P(dbl)]),
+        "mb_torord_initial_state": (i32, [i32, P(dbl)]),
+        "mb_ode_device_state": (i32, [vp, P(vp), P(C.c_size_t)]),
+        "mb_ode_set_steps": (i32, [vp, dbl, C.c_uint32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -90,6 +90,12 @@ int mb_torord_endo_initial_state(int gpu_build, double *state) {
     return MB_OK;
 }
 
+int mb_torord_initial_state(int celltype, double *state) {
+    if (!state || celltype < 0 || celltype > 2) return set_err(MB_ERR_ARG, "bad arguments");
+    for (int s = 0; s < MB_NEQ_TORORD; ++s) state[s] = mb_torord_default_state(celltype, s);
+    return MB_OK;
+}
+
 /* Row counts of the SoA state for (model, precision, adaptive ODE step). */
 static void ode_rows(int model, int precision, int adaptive, int *n64, int *n32) {
     if (model == MB_MODEL_TORORD_FKATP_ENDO) {
@@ -250,6 +256,21 @@ int mb_ode_set_state(mb_ode *o, const double *host_state) {
 /* V of every cell (row 0 of the state) from / to host memory with an
  * element stride: stride = the number of equations reads and writes the
  * reference's array-of-structures state vector (sv[i * neq]) in place. */
+int mb_ode_device_state(mb_ode *o, double **sv, size_t *pitch) {
+    if (!o) return set_err(MB_ERR_ARG, "null ode");
+    if (o->dev.precision != MB_PREC_FP64) return set_err(MB_ERR_ARG, "the device state is pitched FP64 rows only");
+    if (sv) *sv = o->dev.sv64;
+    if (pitch) *pitch = (size_t)o->dev.ld * sizeof(double);
+    return MB_OK;
+}
+
+int mb_ode_set_steps(mb_ode *o, double dt, uint32_t num_steps) {
+    if (!o || !(dt > 0.0) || num_steps == 0) return set_err(MB_ERR_ARG, "bad arguments");
+    o->dev.dt = dt;
+    o->dev.num_steps = (int)num_steps;
+    return MB_OK;
+}
+
 int mb_ode_set_v(mb_ode *o, const double *v, size_t stride) {
     if (!o || !v || stride == 0) return set_err(MB_ERR_ARG, "bad arguments");
     const size_t n = o->dev.n;

@@ -22,12 +22,31 @@
  *     stopping rule as cpu_conjugate_gradient,
  *     linear_system_solver.c:47-183) and writes V back to the cells.
  *
+ * The GPU build of the reference (COMPILE_CUDA, [ode_solver] use_gpu = yes)
+ * resolves the GPU entry points instead (ode_solver.c:114-126) and keeps the
+ * state on the device:
+ *   - set_model_initial_conditions_gpu hands the host this library's own
+ *     device state as ode_solver->sv (pitched FP64 rows, V in row 0, the
+ *     layout of the reference's GPU models, ten_tusscher_2006_RS_GPU.cu:8-40)
+ *     and returns its pitch;
+ *   - solve_model_odes_gpu integrates in place: the host writes V into row 0
+ *     before the call (update_ode_state_vector, monodomain_solver.c:1026-1045)
+ *     and update_monodomain_default reads V* from row 0 after it
+ *     (update_monodomain.c:31-52); nothing crosses to the host.
+ *
+ * ToRORd extra data (set_extra_data_mixed_torord_fkatp_epi_mid_endo and the
+ * like, struct extra_data_for_torord, helper_functions.h:44-68): the cell
+ * type of every cell (transmurality) selects its initial state and its
+ * currents; the initial states must be the reference's default steady states
+ * and every current multiplier 1 (the defaults of set_common_torord_data,
+ * helper_functions.c:94-160) -- other values are reported and fatal.
+ *
  * Compiled against the reference's headers (struct layouts and the plugin
  * signature macros) with CELL_MODEL_REAL_DOUBLE, as the reference's default
  * build; no reference function is called.  MB_SHIM_MODEL selects the cell
  * model this copy provides.  Not supported (reported and fatal, as the
- * reference's fatal paths are): adaptive meshes / cells_to_solve, Purkinje
- * systems, and ToRORd extra data (cell types and current scalings). */
+ * reference's fatal paths are): adaptive meshes / cells_to_solve, the
+ * adaptive ODE step and Purkinje systems. */
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -36,12 +55,13 @@
 
 #include "ode_solver/ode_solver.h"
 #include "config/linear_system_solver_config.h"
+#include "extra_data_library/helper_functions.h"
 #include "3dparty/stb_ds.h"
 
 #include "monoalg3d_b200.h"
 
 #ifndef MB_SHIM_MODEL
-#error "MB_SHIM_MODEL must name the cell model (MB_MODEL_TT2006 or MB_MODEL_TORORD_FKATP_MIXED)"
+#error "MB_SHIM_MODEL must name the cell model (MB_MODEL_TT2006, MB_MODEL_TORORD_FKATP_MIXED or MB_MODEL_TORORD_FKATP_ENDO)"
 #endif
 
 static void shim_fail(const char *what) {
@@ -57,6 +77,46 @@ static void shim_check(int rc, const char *what) {
 
 static mb_ode *g_ode;        /* created at the first solve, when dt and num_steps are final */
 static uint32_t g_ode_cells;
+static uint8_t *g_celltype;  /* ToRORd cell type of every cell (extra data), or NULL */
+
+/* The cell types of the ToRORd extra data, checked against what this library
+ * models (see the header comment); NULL when there is none. */
+static uint8_t *torord_celltypes(struct ode_solver *solver, uint32_t n) {
+    if (MB_SHIM_MODEL != MB_MODEL_TORORD_FKATP_MIXED || !solver->ode_extra_data || solver->extra_data_size == 0)
+        return NULL;
+    const struct extra_data_for_torord *x = (const struct extra_data_for_torord *)solver->ode_extra_data;
+    const real mult[] = {x->INa_Multiplier, x->ICaL_Multiplier, x->Ito_Multiplier, x->INaL_Multiplier,
+                         x->IKr_Multiplier, x->IKs_Multiplier, x->IK1_Multiplier, x->IKb_Multiplier,
+                         x->INaCa_Multiplier, x->INaK_Multiplier, x->INab_Multiplier, x->ICab_Multiplier,
+                         x->IpCa_Multiplier, x->ICaCl_Multiplier, x->IClb_Multiplier, x->Jrel_Multiplier,
+                         x->Jup_Multiplier};
+    for (size_t k = 0; k < sizeof mult / sizeof mult[0]; ++k)
+        if (mult[k] != 1.0) {
+            fprintf(stderr, "monoalg3d_b200 shim: ToRORd current multipliers other than 1 are not supported\n");
+            exit(1);
+        }
+    const real *ic[3] = {x->initial_ss_endo, x->initial_ss_mid, x->initial_ss_epi};
+    double def[43];
+    for (int t = 0; t < 3; ++t) {
+        shim_check(mb_torord_initial_state(t, def), "default initial state");
+        for (int q = 0; q < 43 && ic[t]; ++q)
+            if (ic[t][q] != (real)def[q]) {
+                fprintf(stderr, "monoalg3d_b200 shim: ToRORd initial states other than the default steady "
+                                "states are not supported\n");
+                exit(1);
+            }
+    }
+    uint8_t *ct = (uint8_t *)malloc(n ? n : 1);
+    if (!ct) {
+        fprintf(stderr, "monoalg3d_b200 shim: out of host memory\n");
+        exit(1);
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const real t = x->transmurality ? x->transmurality[i] : 0.0;
+        ct[i] = t == 1.0 ? 1 : (t == 2.0 ? 2 : 0);     /* ENDO 0, MID 1, EPI 2 */
+    }
+    return ct;
+}
 
 GET_CELL_MODEL_DATA(init_cell_model_data) {
     int neq = 0;
@@ -72,11 +132,9 @@ SET_ODE_INITIAL_CONDITIONS_CPU(set_model_initial_conditions_cpu) {
         fprintf(stderr, "monoalg3d_b200 shim: adaptive meshes are not supported\n");
         exit(1);
     }
-    if (MB_SHIM_MODEL == MB_MODEL_TORORD_FKATP_MIXED && solver->ode_extra_data && solver->extra_data_size > 0) {
-        fprintf(stderr, "monoalg3d_b200 shim: ToRORd extra data (cell types, scalings) is not supported\n");
-        exit(1);
-    }
     const uint32_t n = solver->original_num_cells;
+    free(g_celltype);
+    g_celltype = torord_celltypes(solver, n);
     const int neq = solver->model_data.number_of_ode_equations;
     solver->sv = (real *)malloc((size_t)n * neq * sizeof(real));
     double *soa = (double *)malloc((size_t)n * neq * sizeof(double));
@@ -88,7 +146,7 @@ SET_ODE_INITIAL_CONDITIONS_CPU(set_model_initial_conditions_cpu) {
     mb_ode *tmp = NULL;
     size_t pitch = 0;
     shim_check(mb_ode_create(&tmp, MB_SHIM_MODEL, MB_PREC_FP64, MB_RL_REFERENCE_CPU, n, 1.0, 1), "mb_ode_create");
-    shim_check(mb_set_model_initial_conditions_gpu(tmp, NULL, NULL, &pitch), "initial conditions");
+    shim_check(mb_set_model_initial_conditions_gpu(tmp, NULL, g_celltype, &pitch), "initial conditions");
     shim_check(mb_ode_get_state(tmp, soa), "initial state");
     mb_ode_destroy(tmp);
     for (uint32_t i = 0; i < n; ++i)
@@ -116,6 +174,8 @@ SOLVE_MODEL_ODES(solve_model_odes_cpu) {
         shim_check(mb_ode_create(&g_ode, MB_SHIM_MODEL, MB_PREC_FP64, MB_RL_REFERENCE_CPU, n, ode_solver->min_dt,
                                  ode_solver->num_steps),
                    "mb_ode_create");
+        size_t pitch = 0;
+        shim_check(mb_set_model_initial_conditions_gpu(g_ode, NULL, g_celltype, &pitch), "cell types");
         shim_check(mb_ode_set_state(g_ode, soa), "state upload");
         free(soa);
         g_ode_cells = n;
@@ -127,6 +187,41 @@ SOLVE_MODEL_ODES(solve_model_odes_cpu) {
     shim_check(mb_ode_set_v(g_ode, ode_solver->sv, (size_t)neq), "V upload");
     shim_check(mb_solve_model_odes_gpu(g_ode, current_t, stim_currents), "solve_model_odes");
     shim_check(mb_ode_get_v(g_ode, ode_solver->sv, (size_t)neq), "V download");
+}
+
+/* ---- GPU build: the state lives on the device (ode_solver.h:37-47) -------- */
+
+SET_ODE_INITIAL_CONDITIONS_GPU(set_model_initial_conditions_gpu) {
+    (void)ode_extra_config;
+    if (solver->adaptive || solver->cells_to_solve) {
+        fprintf(stderr, "monoalg3d_b200 shim: adaptive meshes and the adaptive ODE step are not supported\n");
+        exit(1);
+    }
+    const uint32_t n = solver->original_num_cells;
+    free(g_celltype);
+    g_celltype = torord_celltypes(solver, n);
+    if (g_ode) mb_ode_destroy(g_ode);
+    /* num_steps is set by the host after this call; the first solve updates it */
+    shim_check(mb_ode_create(&g_ode, MB_SHIM_MODEL, MB_PREC_FP64, MB_RL_REFERENCE_CPU, n, solver->min_dt, 1),
+               "mb_ode_create");
+    size_t pitch = 0;
+    shim_check(mb_set_model_initial_conditions_gpu(g_ode, NULL, g_celltype, &pitch), "initial conditions");
+    double *sv = NULL;
+    shim_check(mb_ode_device_state(g_ode, &sv, &pitch), "device state");
+    solver->sv = (real *)sv;      /* freed by the host with cudaFree at exit (ode_solver.c:45-49) */
+    g_ode_cells = n;
+    return pitch;
+}
+
+SOLVE_MODEL_ODES(solve_model_odes_gpu) {
+    (void)ode_extra_config;
+    if (!g_ode || (uint32_t)ode_solver->num_cells_to_solve != g_ode_cells) {
+        fprintf(stderr, "monoalg3d_b200 shim: solve_model_odes_gpu before set_model_initial_conditions_gpu, or the "
+                        "number of cells changed\n");
+        exit(1);
+    }
+    shim_check(mb_ode_set_steps(g_ode, ode_solver->min_dt, ode_solver->num_steps), "num_steps");
+    shim_check(mb_solve_model_odes_gpu(g_ode, current_t, stim_currents), "solve_model_odes_gpu");
 }
 
 /* ---- linear system solver (linear_system_solver_config.h:12-21) ---------- */

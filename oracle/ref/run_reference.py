@@ -26,6 +26,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF = os.path.join(os.path.dirname(HERE), "_ref")
 BIN = os.path.join(REF, "bin", "MonoAlg3D")
 LIBS = os.path.join(REF, "shared_libs")
+# the reference's GPU build (Makefile.cuda): host loop with COMPILE_CUDA, GPU
+# cell-model kernels, FP32 cuSPARSE / cuBLAS conjugate gradient
+CUDA_BIN = os.path.join(REF, "cuda", "bin", "MonoAlg3D")
+CUDA_LIBS = os.path.join(REF, "cuda", "shared_libs")
 
 MODEL_LIBS = {"tt2006": "libten_tusscher_2006.so", "torord": "libToRORd_fkatp_mixed_endo_mid_epi.so",
               "torord_endo": "libToRORd_fkatp_endo.so"}
@@ -33,6 +37,10 @@ MODEL_LIBS = {"tt2006": "libten_tusscher_2006.so", "torord": "libToRORd_fkatp_mi
 
 def available() -> bool:
     return os.path.exists(BIN) and os.path.exists(os.path.join(LIBS, "libmb_adapters.so"))
+
+
+def cuda_available() -> bool:
+    return os.path.exists(CUDA_BIN) and os.path.exists(os.path.join(CUDA_LIBS, "libmb_adapters.so"))
 
 
 def physical_cores() -> int:
@@ -90,6 +98,8 @@ def ini_text(case: dict, work_dir: str, out_dir: str | None = None, dumps_every:
     transmural extra data, "z_thirds" = the adapter's); stims (list of
     dicts: kind "x_less_than" | "x_y_limits", start, duration, current,
     x_limit | min, max); ecg (dict: leads, sigma_b, calc_rate) or None;
+    use_gpu (the reference's GPU build: ODEs and CG on the GPU) and
+    preconditioner (default True; the GPU CG has none);
     save_state (dict: output_dir, save_rate) and restore_state (dict:
     input_dir) for the reference's checkpoint plugins, or None; dt_ode (ms,
     default dt); adaptive (bool, forward-Euler model "torord_endo") with
@@ -161,7 +171,7 @@ def ini_text(case: dict, work_dir: str, out_dir: str | None = None, dumps_every:
                         f"reltol={case.get('rel_tol', 1e-5)!r}\n")
     stims = case.get("stims") or [dict(kind="x_less_than", start=0.0, duration=2.0, current=-53.0, x_limit=500.0)]
     stim_text = "\n".join(_stim_section(i, s) for i, s in enumerate(stims))
-    return f"""[main]
+    text = f"""[main]
 num_threads={threads}
 dt_pde={dt}
 simulation_time={case['sim_ms']}
@@ -179,10 +189,10 @@ init_function=set_initial_conditions_fvm
 
 [linear_system_solver]
 tolerance=1e-16
-use_preconditioner=yes
+use_preconditioner={'yes' if case.get('preconditioner', True) else 'no'}
 max_iterations=200
 library_file={LIBS}/libdefault_linear_system_solver.so
-use_gpu=no
+use_gpu={'yes' if case.get('use_gpu') else 'no'}
 main_function=conjugate_gradient
 init_function=init_conjugate_gradient
 end_function=end_conjugate_gradient
@@ -199,12 +209,15 @@ side_length_z={nz * dx}
 library_file={LIBS}/{domain_lib}
 
 [ode_solver]
-{ode_dt}{ode_adaptive}use_gpu=no
+{ode_dt}{ode_adaptive}use_gpu={'yes' if case.get('use_gpu') else 'no'}
 gpu_id=0
 library_file={LIBS}/{MODEL_LIBS[case['model']]}
 
 {extra}{stim_text}
 """
+    if case.get("use_gpu"):
+        text = text.replace(f"library_file={LIBS}/", f"library_file={CUDA_LIBS}/")
+    return text
 
 
 # ---- workloads -----------------------------------------------------------------
@@ -300,7 +313,8 @@ def run_case(case: dict, threads: int | None = None, dumps_every: int | None = N
         ini = os.path.join(tmp, "case.ini")
         with open(ini, "w") as f:
             f.write(ini_text(case, tmp, out_dir, dumps_every=dumps_every or 1000000000, threads=threads))
-        log = subprocess.run([BIN, "-c", ini], capture_output=True, text=True, timeout=timeout, check=True).stdout
+        binary = CUDA_BIN if case.get("use_gpu") else BIN
+        log = subprocess.run([binary, "-c", ini], capture_output=True, text=True, timeout=timeout, check=True).stdout
         its, errs = [], []
         for m in re.finditer(r"t = ([0-9.]+), Iterations = (\d+), Error Norm = ([0-9.eE+-]+)", log):
             its.append(int(m.group(2)))
