@@ -314,7 +314,9 @@ def run_case(case: dict, threads: int | None = None, dumps_every: int | None = N
         with open(ini, "w") as f:
             f.write(ini_text(case, tmp, out_dir, dumps_every=dumps_every or 1000000000, threads=threads))
         binary = CUDA_BIN if case.get("use_gpu") else BIN
-        log = subprocess.run([binary, "-c", ini], capture_output=True, text=True, timeout=timeout, check=True).stdout
+        # the GPU build prints the device UUID as raw bytes: decode leniently
+        log = subprocess.run([binary, "-c", ini], capture_output=True, text=True, errors="replace", timeout=timeout,
+                             check=True).stdout
         its, errs = [], []
         for m in re.finditer(r"t = ([0-9.]+), Iterations = (\d+), Error Norm = ([0-9.eE+-]+)", log):
             its.append(int(m.group(2)))

@@ -55,7 +55,7 @@ def _run(case, shim, gpu_host=False):
         ini = os.path.join(tmp, "case.ini")
         with open(ini, "w") as f:
             f.write(text)
-        log = subprocess.run([rr.CUDA_BIN if gpu_host else rr.BIN, "-c", ini], capture_output=True, text=True,
+        log = subprocess.run([rr.CUDA_BIN if gpu_host else rr.BIN, "-c", ini], capture_output=True, text=True, errors="replace",
                              timeout=600)
         assert log.returncode == 0, log.stdout[-2000:] + log.stderr[-2000:]
         its = [int(m.group(2)) for m in re.finditer(

@@ -2,10 +2,12 @@
 (mb_monodomain_save_state / mb_monodomain_restore_state):
 
   - round trip here: a tissue saved after some steps and restored into a new
-    tissue continues bit for bit as the original does, in both state-vector
-    layouts (cell after cell, as the reference's CPU build writes it; state
-    row after state row with the row pitch, as its GPU build does) and in
-    both precisions;
+    tissue holds the same V and continues as the original does, in both
+    state-vector layouts (cell after cell, as the reference's CPU build
+    writes it; state row after state row with the row pitch, as its GPU
+    build does) and in both precisions -- to rounding, since the two
+    tissues' tuners may pick different CG launch shapes (another summation
+    order);
   - the reference's checkpoint, restored here: the reference runs part of
     the simulation and saves; this library restores its files and runs on,
     and matches the reference's uninterrupted run to the end (FP64 bar: 1e-8
@@ -65,7 +67,11 @@ def test_round_trip(tmp_path, cfg, precision, layout):
     va, vb = a.v(), b.v()
     a.close()
     b.close()
-    assert _same(va, vb), f"max |dV| {np.nanmax(np.abs(va - vb)):.3e} mV"
+    assert np.array_equal(np.isfinite(va), np.isfinite(vb))
+    ok = np.isfinite(va)
+    # FP64: rounding; mixed: the FP32 recurrences of another launch shape
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    np.testing.assert_allclose(vb[ok], va[ok], rtol=tol, atol=tol)
 
 
 def test_restore_refuses_another_tissue(tmp_path):
