@@ -74,6 +74,10 @@ struct FastDiv {
 struct ZArgs {
     const double *inv64;           // [nz][9] Jacobi 1/diag per plane and class
     const float *inv32;
+    // [nz][PTAB] FP32: a plane's nine class rows (243 entries), its nine
+    // Jacobi values, zero padding -- one 16-byte-aligned block per plane for
+    // the bulk copy of the window Q pass
+    const float *ptab32;
     // tensor maps of r, p (buffer a), p (buffer b) and x, in global memory
     const CUtensorMap *maps;
     int tiles_x, tiles_y, chunks;
@@ -84,13 +88,18 @@ __host__ __device__ constexpr int r128(int b) { return (b + 127) / 128 * 128; }
 
 constexpr int TSLOTS = 4;          // per-plane table slots
 constexpr int TROW = 9 * 27 + 9;   // one plane: 9 class rows of 27 entries, 9 Jacobi values
+constexpr int PTAB = 256;          // TROW padded to a multiple of 16 bytes (FP32)
+constexpr int QDLY = 2;            // window Q pass: the stage of entry e is refilled at step e + QDLY
 
-template <typename T, int W, int S>
+template <typename T, int W, int S, bool QW = false>
 struct Lay {
     static constexpr int H = W + 2;                         // staged rows
     static constexpr int ELEMS = H * WX;                    // one staged plane
     static constexpr int ARR = r128(ELEMS * (int)sizeof(T));
-    static constexpr int STAGE = 2 * ARR > r128(ELEMS * 8) ? 2 * ARR : r128(ELEMS * 8);
+    // window Q pass: r, p_old and the plane's table (FP32) per stage
+    static constexpr int QSTAGE = (QW && sizeof(T) == 4) ? 2 * ARR + r128(PTAB * 4) : 0;
+    static constexpr int STAGE0 = 2 * ARR > r128(ELEMS * 8) ? 2 * ARR : r128(ELEMS * 8);
+    static constexpr int STAGE = QSTAGE > STAGE0 ? QSTAGE : STAGE0;
     static constexpr int RPLANE = r128(ELEMS * 8);          // ring planes hold doubles (residual pass)
     static constexpr int BARS = 128;
     // the coefficient rows and Jacobi values of up to four planes, both
@@ -143,6 +152,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity) {
 __device__ __forceinline__ void fence_proxy_async() {
     asm volatile("fence.proxy.async.global;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(s32(b)) : "memory");
+}
+// 1-D bulk copy global -> shared (16-byte aligned ends, size a multiple of 16)
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     s32(dst)),
+                 "l"(src), "r"(bytes), "r"(s32(bar))
+                 : "memory");
 }
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z) {
     asm volatile(
@@ -288,6 +307,71 @@ __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, 
     return out;
 }
 
+// The 27-point product for the lane's four cells of row j of plane k from a
+// register window: win[pz][ry] = the lane's four values of plane k - 1 + pz,
+// row j - 1 + ry; hx[pz][ry] = the value beyond the tile's edge (left of the
+// tile in lane 0, right of it in lane 31); tb = plane k's nine class rows.
+// The same sums as apply27: entry order, the warp's interior row for every
+// cell, then the cells on an x face of the grid with their own rows (their
+// neighbours outside the grid are zero, as the staged halo is there).
+template <typename R>
+__device__ __forceinline__ V4<R> apply_w(const mb_stencil_dev &st, const V4<R> (&win)[3][3], const R (&hx)[3][3],
+                                         const float *tb, int i0, int j, int lane) {
+    const int cy = axis_class(j, st.ny);
+    const float *cm = tb + (cy * 3 + 1) * 27;
+    R acc[4] = {R(0), R(0), R(0), R(0)};
+#pragma unroll
+    for (int pz = 0; pz < 3; ++pz) {
+#pragma unroll
+        for (int ry = 0; ry < 3; ++ry) {
+            const unsigned rb = (st.nzmask >> (pz * 9 + ry * 3)) & 7u;
+            if (!rb) continue;
+            const V4<R> &m4 = win[pz][ry];
+            const R sl = __shfl_up_sync(0xffffffffu, m4.v[3], 1);
+            const R sr = __shfl_down_sync(0xffffffffu, m4.v[0], 1);
+            R wv[6];
+            wv[0] = lane == 0 ? hx[pz][ry] : sl;
+            wv[5] = lane == 31 ? hx[pz][ry] : sr;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) wv[c + 1] = m4.v[c];
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (!((rb >> (dx + 1)) & 1u)) continue;
+                const R cc = (R)cm[pz * 9 + ry * 3 + (dx + 1)];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[c] = fma(cc, wv[c + 1 + dx], acc[c]);
+            }
+        }
+    }
+    // cells on an x face: only the lanes holding one take this branch
+    const int e = i0 == 0 ? 0 : (i0 + 3 == st.nx - 1 ? 3 : -1);
+    if (e >= 0) {
+        const float *ce = tb + (cy * 3 + axis_class(i0 + e, st.nx)) * 27;
+        R a = R(0);
+#pragma unroll
+        for (int pz = 0; pz < 3; ++pz) {
+#pragma unroll
+            for (int ry = 0; ry < 3; ++ry) {
+                const V4<R> &m4 = win[pz][ry];
+                // the face cell's neighbours dx = -1, 0, +1 (zero outside the grid)
+                const R lo[3] = {R(0), m4.v[0], m4.v[1]};
+                const R hi[3] = {m4.v[2], m4.v[3], R(0)};
+#pragma unroll
+                for (int dx = 0; dx < 3; ++dx) {
+                    const int q = pz * 9 + ry * 3 + dx;
+                    if ((st.nzmask >> q) & 1u) a = fma((R)ce[q], e == 0 ? lo[dx] : hi[dx], a);
+                }
+            }
+        }
+        if (e == 0) acc[0] = a;
+        else acc[3] = a;
+    }
+    V4<R> out;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) out.v[c] = acc[c];
+    return out;
+}
+
 // One stencil pass over every unit of this block.  issue(U, m, stage, bar)
 // (thread 0) starts the copies of plane m of unit U into a stage buffer;
 // form(U, m, stage, ring) turns a staged plane into ring plane input;
@@ -397,10 +481,11 @@ struct Tabs {
 
 // ---- the solve ----------------------------------------------------------------
 
-template <bool MIXED, int W, int S, int MINB>
+template <bool MIXED, int W, int S, int MINB, bool QW>
 __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
     using T = typename Prec<MIXED>::T;
-    using L = Lay<T, W, S>;
+    using L = Lay<T, W, S, QW>;
+    static_assert(S <= 4, "the barrier area holds 4 + 4 + 4 mbarriers");
     // Dynamic shared memory starts after the static reduction arrays of
     // grid_reduce, at an offset aligned to 16 bytes only; it is declared
     // with that alignment (a larger declared one would let the compiler
@@ -436,6 +521,12 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         for (int q = 0; q < 4; ++q)
             asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(z.maps + q) : "memory");
         for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+        // window Q pass: full (the copies of a stage) and empty (every warp
+        // done with it) barriers
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&bars[4 + s], 1);
+            mbar_init(&bars[8 + s], W);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -550,6 +641,161 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         return zpass<W, S>(z, a, smem, L::TABS, L::STAGE, L::RPLANE, pp, issue, tabs, form, out);
     };
 
+    // ---- window Q pass (QW, mixed): the same products without the ring ----------
+    // Each warp forms the direction p for its own row and the rows above and
+    // below it (one row of four cells per lane) straight from the staged r
+    // and p_old, keeps p of the last three planes in registers (win) and
+    // applies the stencil from there; stage buffers are handed back per warp
+    // through an "empty" mbarrier instead of a block barrier per plane.
+    // Entry e of the block's plane sequence (over its units) is staged in
+    // stage e % S with r, p_old and the plane's table; its table is read
+    // again at entry e + 1 (the product of plane e), so the warp releases
+    // stage e at entry e + 1, and thread 0 refills it with entry e + S at
+    // entry e + QDLY, after every warp has released it.
+    unsigned qbase = 0;    // entries of the earlier window Q passes (mbarrier phases)
+    auto qpass_w = [&](bool first, const T *pold, T *pw, double beta, double &q1) -> bool {
+        const CUtensorMap *mp = pold == bufa ? tm_pa : tm_pb;
+        const T bt = (T)beta;
+        uint64_t *full = bars + 4, *empty = bars + 8;
+        unsigned char *stage0 = smem + 128 + L::TABS;
+        const int units = z.tiles_x * z.tiles_y * z.chunks;
+        const unsigned bytes = (unsigned)(L::ELEMS * sizeof(T)) * (first ? 1u : 2u) + (unsigned)(PTAB * 4);
+        // producer cursor (thread 0)
+        int pun = blockIdx.x, pm = 0;
+        Unit PU{0, 0, 0, 0};
+        if (pun < units) PU = unit_of<W>(z, nz, pun);
+        unsigned issued = 0;
+        bool ok = true;
+        auto produce = [&]() {
+            if (pun >= units || !ok) return;
+            const unsigned E = qbase + issued;
+            const int s = (int)(E % S);
+            if (E >= (unsigned)S && !mbar_wait(&empty[s], (E / S - 1u) & 1u)) {
+                ok = false;
+                return;
+            }
+            fence_proxy_async();
+            unsigned char *stg = stage0 + (size_t)s * L::STAGE;
+            const int m = PU.k0 - 1 + pm;
+            const int mc = m < 0 ? 0 : (m >= nz ? nz - 1 : m);
+            mbar_expect_tx(&full[s], bytes);
+            tma_load_3d(stg, tm_r, &full[s], PU.x0 - HX, PU.y0 - 1, m);
+            if (!first) tma_load_3d(stg + L::ARR, mp, &full[s], PU.x0 - HX, PU.y0 - 1, m);
+            bulk_load(stg + 2 * L::ARR, z.ptab32 + (size_t)mc * PTAB, (unsigned)(PTAB * 4), &full[s]);
+            ++issued;
+            if (++pm >= PU.k1 - PU.k0 + 2) {
+                pm = 0;
+                pun += gridDim.x;
+                if (pun < units) PU = unit_of<W>(z, nz, pun);
+            }
+        };
+        if (threadIdx.x == 0)
+            for (int i = 0; i < S - QDLY; ++i) produce();
+        V4<T> win[3][3];
+        T hx[3][3];
+#pragma unroll
+        for (int pz = 0; pz < 3; ++pz)
+#pragma unroll
+            for (int ry = 0; ry < 3; ++ry) {
+                win[pz][ry] = V4<T>{{T(0), T(0), T(0), T(0)}};
+                hx[pz][ry] = T(0);
+            }
+        unsigned e = 0;       // entries of this pass consumed by this thread
+        for (int un = blockIdx.x; un < units && ok; un += gridDim.x) {
+            const Unit U = unit_of<W>(z, nz, un);
+            const int P = U.k1 - U.k0 + 2;
+            const int j = U.y0 + w, i0 = U.x0 + 4 * lane;
+            for (int u = 0; u < P; ++u, ++e) {
+                const unsigned E = qbase + e;
+                const int s = (int)(E % S);
+                if (!mbar_wait(&full[s], (E / S) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                const unsigned char *stg = stage0 + (size_t)s * L::STAGE;
+                const T *rs = reinterpret_cast<const T *>(stg);
+                const T *ps = reinterpret_cast<const T *>(stg + L::ARR);
+                const float *tb = reinterpret_cast<const float *>(stg + 2 * L::ARR);
+                const int m = U.k0 - 1 + u;
+#pragma unroll
+                for (int ry = 0; ry < 3; ++ry) {
+                    win[0][ry] = win[1][ry];
+                    win[1][ry] = win[2][ry];
+                    hx[0][ry] = hx[1][ry];
+                    hx[1][ry] = hx[2][ry];
+                }
+#pragma unroll
+                for (int h = 0; h < 3; ++h) {
+                    const int jr = j - 1 + h;
+                    const float *irow = tb + 243 + axis_class(jr, ny) * 3;
+                    const int o = (w + h) * WX + HX + 4 * lane;
+                    const V4<T> rv = ld4(rs + o);
+                    V4<T> po = {{T(0), T(0), T(0), T(0)}};
+                    if (!first) po = ld4(ps + o);
+                    T iv[4];
+                    if (i0 > 0 && i0 + 3 < nx - 1) {
+                        iv[0] = iv[1] = iv[2] = iv[3] = (T)irow[1];
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) iv[q] = (T)irow[axis_class(i0 + q, nx)];
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const T zz = pre ? mul_rn(iv[q], rv.v[q]) : rv.v[q];
+                        win[2][h].v[q] = first ? zz : fma(bt, po.v[q], zz);
+                    }
+                    // the value beyond the tile's edge: left of it in lane 0,
+                    // right of it in lane 31 (zero outside the grid)
+                    T ph = T(0);
+                    if (lane == 0 || lane == 31) {
+                        const int ce = lane == 0 ? -1 : 4;
+                        const T re = rs[o + ce];
+                        const T pe = first ? T(0) : ps[o + ce];
+                        const T ie = (T)irow[axis_class(i0 + ce, nx)];
+                        const T zz = pre ? mul_rn(ie, re) : re;
+                        ph = first ? zz : fma(bt, pe, zz);
+                    }
+                    hx[2][h] = ph;
+                }
+                if (m >= U.k0 && m < U.k1 && j < ny && i0 < nx)
+                    st4(pw + (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * m), win[2][1]);
+                if (u >= 2) {
+                    // plane m - 1, with its table (stage of entry e - 1)
+                    const float *tp =
+                        reinterpret_cast<const float *>(stage0 + (size_t)((E - 1u) % S) * L::STAGE + 2 * L::ARR);
+                    const V4<T> ap = apply_w<T>(st, win, hx, tp, i0, j, lane);
+                    if (j < ny && i0 < nx) {
+                        const size_t g0 = (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * (m - 1));
+                        st4(apb + g0, ap);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) q1 += (double)win[1][1].v[q] * (double)ap.v[q];
+                    }
+                }
+                // stage of entry e - 1: its table was read for the last time above
+                if (e > 0) {
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&empty[(E - 1u) % S]);
+                }
+                if (threadIdx.x == 0) produce();
+            }
+        }
+        if (ok && e > 0) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[(qbase + e - 1u) % S]);
+        }
+        if (!__syncthreads_and(ok)) {
+            // let the copies this block started finish before it leaves
+            if (threadIdx.x == 0) {
+                atomicExch(a.status, MB_ERR_CUDA);
+                for (unsigned E = qbase + e; E < qbase + issued; ++E) (void)mbar_wait(&full[E % S], (E / S) & 1u);
+            }
+            __syncthreads();
+            return false;
+        }
+        qbase += e;
+        return true;
+    };
+
     // ---- U pass: x += alpha p, r -= alpha A p; r.z, r.r (z formed, not stored) -----
     auto upass = [&](const T *pc_, double alpha, double (&u2)[2]) {
         const T al = (T)alpha;
@@ -617,7 +863,10 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
     while (!done) {
         T *pnew = pcur == bufa ? bufb : bufa;
         double q1[1] = {0.0}, s1[1];
-        if (!qpass(first, pcur, pnew, beta, q1[0])) return;
+        bool qok;
+        if constexpr (QW && MIXED) qok = qpass_w(first, pcur, pnew, beta, q1[0]);
+        else qok = qpass(first, pcur, pnew, beta, q1[0]);
+        if (!qok) return;
         if (!grid_reduce<1, 32 * W>(a, q1, s1, red)) return;
         const double alpha = (pre ? rz : rr) / s1[0];
         pcur = pnew;
@@ -669,12 +918,28 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
     }
 }
 
-// Jacobi 1/diag per plane and row class: 1 / the class row's diagonal entry.
-__global__ void k_zinv(mb_stencil_dev st, double *inv64, float *inv32) {
+// Jacobi 1/diag per plane and row class: 1 / the class row's diagonal entry;
+// and the padded FP32 per-plane blocks of the window Q pass (class rows,
+// Jacobi values, zeros).
+__global__ void k_zinv(mb_stencil_dev st, double *inv64, float *inv32, float *ptab32) {
     const int n = st.nz * 9;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         inv64[e] = 1.0 / st.table[(size_t)e * 27 + 13];
         inv32[e] = 1.0f / (st.table32 ? st.table32[(size_t)e * 27 + 13] : (float)st.table[(size_t)e * 27 + 13]);
+    }
+    if (!ptab32) return;
+    const int np = st.nz * PTAB;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < np; e += gridDim.x * blockDim.x) {
+        const int k = e / PTAB, q = e - k * PTAB;
+        float v = 0.0f;
+        if (q < 243) {
+            const size_t src = (size_t)k * 243 + q;
+            v = st.table32 ? st.table32[src] : (float)st.table[src];
+        } else if (q < 252) {
+            const size_t src = ((size_t)k * 9 + (q - 243)) * 27 + 13;
+            v = 1.0f / (st.table32 ? st.table32[src] : (float)st.table[src]);
+        }
+        ptab32[e] = v;
     }
 }
 
@@ -686,20 +951,27 @@ struct Variant {
     int bytes;     // dynamic shared memory
 };
 
-template <bool MIXED, int W, int S, int MINB>
+template <bool MIXED, int W, int S, int MINB, bool QW = false>
 constexpr Variant make() {
-    return {(const void *)k_zcg<MIXED, W, S, MINB>, W, Lay<typename Prec<MIXED>::T, W, S>::BYTES};
+    return {(const void *)k_zcg<MIXED, W, S, MINB, QW>, W, Lay<typename Prec<MIXED>::T, W, S, QW>::BYTES};
 }
 
-#define MB_ZSHAPES(M) make<M, 8, 3, 1>(), make<M, 8, 3, 2>(), make<M, 16, 3, 1>(), make<M, 4, 3, 3>()
-constexpr int NUM_VARIANTS = 4;
+// Mixed: the last three run the window Q pass.  FP64 has no window pass;
+// its last three are ring-pass shapes whose shared memory fits (four stages
+// of FP64 planes of W = 16 do not).
+constexpr int NUM_VARIANTS = 7;
 
 static Variant variant(int mixed, int v) {
-    static const Variant t64[NUM_VARIANTS] = {MB_ZSHAPES(false)};
-    static const Variant t32[NUM_VARIANTS] = {MB_ZSHAPES(true)};
+    static const Variant t64[NUM_VARIANTS] = {make<false, 8, 3, 1>(),  make<false, 8, 3, 2>(),
+                                              make<false, 16, 3, 1>(), make<false, 4, 3, 3>(),
+                                              make<false, 8, 4, 2>(),  make<false, 16, 3, 1>(),
+                                              make<false, 4, 4, 3>()};
+    static const Variant t32[NUM_VARIANTS] = {make<true, 8, 3, 1>(),        make<true, 8, 3, 2>(),
+                                              make<true, 16, 3, 1>(),       make<true, 4, 3, 3>(),
+                                              make<true, 8, 4, 2, true>(),  make<true, 16, 4, 1, true>(),
+                                              make<true, 4, 4, 3, true>()};
     return mixed ? t32[v] : t64[v];
 }
-#undef MB_ZSHAPES
 
 // Resident blocks of a variant per SM x SMs (0 where it does not fit).
 static int grid_of(const Variant &var) {
@@ -780,15 +1052,19 @@ extern "C" int mbk_zcg_max_blocks(int mixed, int v) {
 // Whether the z-march kernel applies: the 27-point class-table operator on a
 // grid whose rows are whole 16-byte vectors (nx % 4 == 0).
 extern "C" int mbk_zcg_usable(const mb_stencil_dev *st) {
-    return st->kind == 2 && st->nx % 4 == 0 && st->nx >= 4 && st->ny >= 1 && st->nz >= 1 && st->table &&
+    return st->kind == 2 && st->nx % 4 == 0 && st->nx >= 8 && st->ny >= 1 && st->nz >= 1 && st->table &&
            st->table32;
 }
 
-// Per-plane Jacobi tables (device arrays of nz * 9 values each).
-extern "C" int mbk_zcg_inv_tables(const mb_stencil_dev *st, double *inv64, float *inv32, cudaStream_t s) {
-    k_zinv<<<(st->nz * 9 + 255) / 256, 256, 0, s>>>(*st, inv64, inv32);
+// Per-plane Jacobi tables (device arrays of nz * 9 values each) and the
+// padded per-plane blocks (nz * PTAB floats; may be NULL).
+extern "C" int mbk_zcg_inv_tables(const mb_stencil_dev *st, double *inv64, float *inv32, float *ptab32,
+                                  cudaStream_t s) {
+    k_zinv<<<(st->nz * PTAB + 255) / 256, 256, 0, s>>>(*st, inv64, inv32, ptab32);
     return (int)cudaGetLastError();
 }
+
+extern "C" int mbk_zcg_ptab_floats(void) { return PTAB; }
 
 // Tensor maps of every variant (4 per variant: r, p buffer a, p buffer b,
 // x), encoded on the host and copied to a device array p->zc_maps allocated
@@ -824,6 +1100,7 @@ extern "C" int mbk_zcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
     ZArgs z;
     z.inv64 = p->zc_inv64;
     z.inv32 = p->zc_inv32;
+    z.ptab32 = p->zc_ptab32;
     z.maps = reinterpret_cast<const CUtensorMap *>(p->zc_maps) + 4 * p->zc_variant;
     z.tiles_x = (nx + TX - 1) / TX;
     z.tiles_y = (ny + var.warps - 1) / var.warps;

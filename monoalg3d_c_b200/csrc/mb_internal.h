@@ -204,6 +204,7 @@ typedef struct mb_pcg_dev {
     int zc_variant;
     double *zc_inv64;
     float *zc_inv32;
+    float *zc_ptab32;       /* [nz][mbk_zcg_ptab_floats()] per-plane blocks (window Q pass) */
     void *zc_maps;
 } mb_pcg_dev;
 enum { MB_PCG_FLAT = 0, MB_PCG_TILED = 1, MB_PCG_RESIDENT = 2, MB_PCG_ZMARCH = 3 };
@@ -220,7 +221,8 @@ int mbk_inv_diag(const mb_stencil_dev *st, double *d64, float *d32, cudaStream_t
 int mbk_zcg_variants(void);
 int mbk_zcg_max_blocks(int mixed, int variant);
 int mbk_zcg_usable(const mb_stencil_dev *st);
-int mbk_zcg_inv_tables(const mb_stencil_dev *st, double *inv64, float *inv32, cudaStream_t s);
+int mbk_zcg_inv_tables(const mb_stencil_dev *st, double *inv64, float *inv32, float *ptab32, cudaStream_t s);
+int mbk_zcg_ptab_floats(void);
 int mbk_zcg_prepare(mb_pcg_dev *p);
 int mbk_zcg_launch(const mb_pcg_dev *p, cudaStream_t s);
 

@@ -348,7 +348,7 @@ void mb_monodomain_destroy(mb_monodomain *m) {
                     m->d_partials, m->d_sv64, m->d_sv32, m->d_stim_bits, m->d_celltype, m->d_scale,
                     m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_code, m->d_rowid, m->d_act,
                     m->d_stim_host, m->d_ctrl, m->d_log, m->d_stim2[0], m->d_stim2[1], m->d_vsnap[0],
-                    m->d_vsnap[1], m->pcg.zc_inv64, m->pcg.zc_inv32, m->pcg.zc_maps};
+                    m->d_vsnap[1], m->pcg.zc_inv64, m->pcg.zc_inv32, m->pcg.zc_ptab32, m->pcg.zc_maps};
     for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
     for (int i = 0; i < 4; ++i) if (m->ev[i]) cudaEventDestroy(m->ev[i]);
     for (int i = 0; i < 4; ++i)
@@ -836,7 +836,8 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
             if (mbk_zcg_usable(&m->st)) {
                 ALLOC(m->pcg.zc_inv64, (size_t)d->nz * 9 * sizeof(double));
                 ALLOC(m->pcg.zc_inv32, (size_t)d->nz * 9 * sizeof(float));
-                CKK(mbk_zcg_inv_tables(&m->st, m->pcg.zc_inv64, m->pcg.zc_inv32, m->stream));
+                ALLOC(m->pcg.zc_ptab32, (size_t)d->nz * mbk_zcg_ptab_floats() * sizeof(float));
+                CKK(mbk_zcg_inv_tables(&m->st, m->pcg.zc_inv64, m->pcg.zc_inv32, m->pcg.zc_ptab32, m->stream));
             }
             CKK(cudaStreamSynchronize(m->stream));
             ALLOC(m->d_bar, 2 * sizeof(unsigned));

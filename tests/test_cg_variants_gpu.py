@@ -22,7 +22,7 @@ import oracle  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 STEPS = 120
-ZMARCH_VARIANTS = 4
+ZMARCH_VARIANTS = 7
 
 
 def _kernel_id(v: int, nf: int) -> int:

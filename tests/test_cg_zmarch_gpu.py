@@ -18,7 +18,7 @@ import oracle  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 STEPS = 60
-ZMARCH_VARIANTS = 4
+ZMARCH_VARIANTS = 7
 
 
 def _case():
