@@ -659,7 +659,25 @@ __global__ void __launch_bounds__(CG_THREADS) k_csr_dir(CsrArgs a) {
 
 using namespace mb;
 
-extern "C" int mbk_max_grid_blocks(void) { return 148 * 8; }
+// Blocks of the graph-form CG kernels and the CSR kernels' partial-sum
+// arrays: 8 per SM of the current device (looked up once per device).
+extern "C" int mbk_max_grid_blocks(void) {
+    static int per_device[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 148 * 8;
+    }
+    if (!per_device[dev]) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+            cudaGetLastError();
+            sms = 148;
+        }
+        per_device[dev] = sms * 8;
+    }
+    return per_device[dev];
+}
 
 extern "C" int mbk_cg_init(const mb_stencil_dev *st, const mb_cg_dev *cg, mb_ctrl *ctrl, unsigned long long cond,
                            int use_cond, cudaStream_t s) {

@@ -74,9 +74,9 @@ struct FastDiv {
 struct ZArgs {
     const double *inv64;           // [nz][9] Jacobi 1/diag per plane and class
     const float *inv32;
-    // [nz][PTAB] FP32: a plane's nine class rows (243 entries), its nine
-    // Jacobi values, zero padding -- one 16-byte-aligned block per plane for
-    // the bulk copy of the window Q pass
+    // [nz][PTAB] FP32: a plane's nine class rows (padded to CROW entries),
+    // its nine Jacobi values at JOFF, zero padding -- one 16-byte-aligned
+    // block per plane for the bulk copy of the window Q pass
     const float *ptab32;
     // tensor maps of r, p (buffer a), p (buffer b) and x, in global memory
     const CUtensorMap *maps;
@@ -87,8 +87,15 @@ struct ZArgs {
 __host__ __device__ constexpr int r128(int b) { return (b + 127) / 128 * 128; }
 
 constexpr int TSLOTS = 4;          // per-plane table slots
-constexpr int TROW = 9 * 27 + 9;   // one plane: 9 class rows of 27 entries, 9 Jacobi values
-constexpr int PTAB = 256;          // TROW padded to a multiple of 16 bytes (FP32)
+constexpr int TROW = 9 * 27 + 9;   // one plane in global memory: 9 class rows of 27 entries, 9 Jacobi values
+// In shared memory each class row is padded to CROW entries, so that a row
+// starts on a 16-byte boundary and its coefficients load as vectors (one
+// broadcast wavefront per four FP32 / two FP64 entries); the Jacobi values
+// follow at JOFF.
+constexpr int CROW = 28;
+constexpr int JOFF = 9 * CROW;
+constexpr int TSLOT = JOFF + 12;   // entries per plane slot (a multiple of 4)
+constexpr int PTAB = TSLOT;        // the same block in global memory (FP32, 16-byte multiple)
 constexpr int QDLY = 2;            // window Q pass: the stage of entry e is refilled at step e + QDLY
 
 template <typename T, int W, int S, bool QW = false>
@@ -104,7 +111,7 @@ struct Lay {
     static constexpr int BARS = 128;
     // the coefficient rows and Jacobi values of up to four planes, both
     // precisions (the residual pass applies the FP64 rows)
-    static constexpr int TABS = r128(TSLOTS * TROW * 8) + r128(TSLOTS * TROW * 4);
+    static constexpr int TABS = r128(TSLOTS * TSLOT * 8) + r128(TSLOTS * TSLOT * 4);
     // + 128: the dynamic shared memory base is aligned up to 128 bytes at run
     // time (bulk tensor copies write to 128-byte-aligned shared addresses)
     static constexpr int BYTES = BARS + TABS + S * STAGE + RING * RPLANE + 128;
@@ -242,19 +249,49 @@ struct Pipe {
     uint32_t phase;
 };
 
+// A class row (CROW entries, 16-byte aligned, in shared memory) into registers
+// by vector loads.
+__device__ __forceinline__ void load_row(const float *row, float (&cc)[CROW]) {
+#pragma unroll
+    for (int q = 0; q < CROW; q += 4) {
+        const float4 v = *reinterpret_cast<const float4 *>(row + q);
+        cc[q] = v.x;
+        cc[q + 1] = v.y;
+        cc[q + 2] = v.z;
+        cc[q + 3] = v.w;
+    }
+}
+__device__ __forceinline__ void load_row(const double *row, double (&cc)[CROW]) {
+#pragma unroll
+    for (int q = 0; q < CROW; q += 2) {
+        const double2 v = *reinterpret_cast<const double2 *>(row + q);
+        cc[q] = v.x;
+        cc[q + 1] = v.y;
+    }
+}
+
 // The 27-point product for the lane's four cells of row j, from ring planes
 // lo (k-1), mid (k), hi (k+1) (row stride WX, staged row h = the tile row +
 // 1) and the plane's class rows ct (9 rows of 27 entries in shared memory).
 // Every cell is first summed with the row of its y class and the interior x
 // class (the same row for the whole warp); lanes holding a cell on an x face
-// (i = 0 or nx - 1) then redo that cell with its own row.  Entries that are
-// zero in every row (st.nzmask) are skipped; sums run in entry order.  All 32
-// lanes call it together.
-template <typename R, int W>
+// (i = 0 or nx - 1) then redo that cell with its own row.  Sums run in entry
+// order.  DENSE: every one of the 27 entries is applied -- the table holds
+// zeros where the operator has none, and fma(0, v, s) = s, so the sums are
+// those of the sparse form -- as straight-line code whose shared loads the
+// compiler can issue ahead of the arithmetic (measured faster than skipping
+// the entries that are zero in every row, st.nzmask, in both precisions).
+// All 32 lanes call it together.
+template <typename R, int W, bool DENSE = true>
 __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, const R *mid, const R *hi,
                                          const R *ct, int i0, int j, int w, int lane) {
     const int cy = axis_class(j, st.ny);
-    const R *cm = ct + (cy * 3 + 1) * 27;
+    const R *cm = ct + (cy * 3 + 1) * CROW;
+    const uint32_t mask = DENSE ? 0x7ffffffu : st.nzmask;
+    // FP32: the row in registers, loaded as vectors; FP64 reads each entry
+    // where it is used (its 28 values would take 56 registers)
+    R cc[sizeof(R) == 4 ? CROW : 1];
+    if constexpr (sizeof(R) == 4) load_row(cm, cc);
     R acc[4] = {R(0), R(0), R(0), R(0)};
     const int off = HX + 4 * lane;
 #pragma unroll
@@ -262,13 +299,16 @@ __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, 
         const R *pl = dz < 0 ? lo : (dz == 0 ? mid : hi);
 #pragma unroll
         for (int dy = -1; dy <= 1; ++dy) {
-            const unsigned rb = (st.nzmask >> ((dz + 1) * 9 + (dy + 1) * 3)) & 7u;
+            const unsigned rb = (mask >> ((dz + 1) * 9 + (dy + 1) * 3)) & 7u;
             if (!rb) continue;
             const R *rowp = pl + (w + 1 + dy) * WX + off;
             const V4<R> m4 = ld4(rowp);
             const R sl = __shfl_up_sync(0xffffffffu, m4.v[3], 1);
             const R sr = __shfl_down_sync(0xffffffffu, m4.v[0], 1);
             R wv[6];
+            // the values beyond the tile's row (a select, not a branch: a
+            // branch per row keeps the compiler from scheduling the rows'
+            // loads ahead, measured slower)
             wv[0] = lane == 0 ? rowp[-1] : sl;
             wv[5] = lane == 31 ? rowp[4] : sr;
 #pragma unroll
@@ -277,16 +317,18 @@ __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, 
             for (int dx = -1; dx <= 1; ++dx) {
                 if (!((rb >> (dx + 1)) & 1u)) continue;
                 const int q = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-                const R cc = cm[q];
+                R cq;
+                if constexpr (sizeof(R) == 4) cq = cc[q];
+                else cq = cm[q];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) acc[c] = fma(cc, wv[c + 1 + dx], acc[c]);
+                for (int c = 0; c < 4; ++c) acc[c] = fma(cq, wv[c + 1 + dx], acc[c]);
             }
         }
     }
     // cells on an x face: only the lanes holding one take this branch
     const int e = i0 == 0 ? 0 : (i0 + 3 == st.nx - 1 ? 3 : -1);
     if (e >= 0) {
-        const R *ce = ct + (cy * 3 + axis_class(i0 + e, st.nx)) * 27;
+        const R *ce = ct + (cy * 3 + axis_class(i0 + e, st.nx)) * CROW;
         R a = R(0);
         for (int dz = -1; dz <= 1; ++dz) {
             const R *pl = dz < 0 ? lo : (dz == 0 ? mid : hi);
@@ -294,7 +336,7 @@ __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, 
                 const R *rowp = pl + (w + 1 + dy) * WX + off + e;
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int q = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-                    if ((st.nzmask >> q) & 1u) a = fma(ce[q], rowp[dx], a);
+                    if ((mask >> q) & 1u) a = fma(ce[q], rowp[dx], a);
                 }
             }
         }
@@ -318,13 +360,15 @@ template <typename R>
 __device__ __forceinline__ V4<R> apply_w(const mb_stencil_dev &st, const V4<R> (&win)[3][3], const R (&hx)[3][3],
                                          const float *tb, int i0, int j, int lane) {
     const int cy = axis_class(j, st.ny);
-    const float *cm = tb + (cy * 3 + 1) * 27;
+    float cc[CROW];
+    load_row(tb + (cy * 3 + 1) * CROW, cc);
+    const uint32_t mask = 0x7ffffffu;      // dense, as apply27 in FP32
     R acc[4] = {R(0), R(0), R(0), R(0)};
 #pragma unroll
     for (int pz = 0; pz < 3; ++pz) {
 #pragma unroll
         for (int ry = 0; ry < 3; ++ry) {
-            const unsigned rb = (st.nzmask >> (pz * 9 + ry * 3)) & 7u;
+            const unsigned rb = (mask >> (pz * 9 + ry * 3)) & 7u;
             if (!rb) continue;
             const V4<R> &m4 = win[pz][ry];
             const R sl = __shfl_up_sync(0xffffffffu, m4.v[3], 1);
@@ -337,16 +381,16 @@ __device__ __forceinline__ V4<R> apply_w(const mb_stencil_dev &st, const V4<R> (
 #pragma unroll
             for (int dx = -1; dx <= 1; ++dx) {
                 if (!((rb >> (dx + 1)) & 1u)) continue;
-                const R cc = (R)cm[pz * 9 + ry * 3 + (dx + 1)];
+                const R c0 = (R)cc[pz * 9 + ry * 3 + (dx + 1)];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) acc[c] = fma(cc, wv[c + 1 + dx], acc[c]);
+                for (int c = 0; c < 4; ++c) acc[c] = fma(c0, wv[c + 1 + dx], acc[c]);
             }
         }
     }
     // cells on an x face: only the lanes holding one take this branch
     const int e = i0 == 0 ? 0 : (i0 + 3 == st.nx - 1 ? 3 : -1);
     if (e >= 0) {
-        const float *ce = tb + (cy * 3 + axis_class(i0 + e, st.nx)) * 27;
+        const float *ce = tb + (cy * 3 + axis_class(i0 + e, st.nx)) * CROW;
         R a = R(0);
 #pragma unroll
         for (int pz = 0; pz < 3; ++pz) {
@@ -359,7 +403,7 @@ __device__ __forceinline__ V4<R> apply_w(const mb_stencil_dev &st, const V4<R> (
 #pragma unroll
                 for (int dx = 0; dx < 3; ++dx) {
                     const int q = pz * 9 + ry * 3 + dx;
-                    if ((st.nzmask >> q) & 1u) a = fma((R)ce[q], e == 0 ? lo[dx] : hi[dx], a);
+                    a = fma((R)ce[q], e == 0 ? lo[dx] : hi[dx], a);
                 }
             }
         }
@@ -472,8 +516,10 @@ struct Tabs {
         for (int i = 0; i < PER; ++i) {
             const int e = threadIdx.x + NT * i;
             if (e < TROW) {
-                tab64[slot * TROW + e] = h64[i];
-                tab32[slot * TROW + e] = h32[i];
+                const int row = e / 27;
+                const int d = e < 243 ? row * CROW + (e - row * 27) : JOFF + (e - 243);
+                tab64[slot * TSLOT + d] = h64[i];
+                tab32[slot * TSLOT + d] = h32[i];
             }
         }
     }
@@ -537,11 +583,11 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
     // nine class rows (27 entries each) and then its nine Jacobi values, in
     // FP64 (tab64) and FP32 (tab32)
     double *tab64 = reinterpret_cast<double *>(smem + 128);
-    float *tab32 = reinterpret_cast<float *>(smem + 128 + r128(TSLOTS * TROW * 8));
+    float *tab32 = reinterpret_cast<float *>(smem + 128 + r128(TSLOTS * TSLOT * 8));
     Tabs<32 * W> tabs{tab64, tab32, st.table, st.table32, z.inv64, z.inv32, nz};
     auto tabT = [&](int slot) -> const T * {
-        if constexpr (sizeof(T) == 8) return tab64 + slot * TROW;
-        else return tab32 + slot * TROW;
+        if constexpr (sizeof(T) == 8) return tab64 + slot * TSLOT;
+        else return tab32 + slot * TSLOT;
     };
 
     // ---- residual pass: r = b - A x (FP64), partials r.z, r.r, r64.r64 ----------
@@ -558,13 +604,13 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         auto out = [&](const Unit &U, int k, int ts, unsigned char *lo, unsigned char *mid, unsigned char *hi) {
             const int j = U.y0 + w, i0 = U.x0 + 4 * lane;
             if (j >= ny) return;                     // warp-uniform
-            const double *ct = tab64 + ts * TROW;
+            const double *ct = tab64 + ts * TSLOT;
             const V4<double> ax = apply27<double, W>(st, reinterpret_cast<const double *>(lo),
                                                      reinterpret_cast<const double *>(mid),
                                                      reinterpret_cast<const double *>(hi), ct, i0, j, w, lane);
             if (i0 >= nx) return;
             const size_t g0 = (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * k);
-            const T *iv = tabT(ts) + 243 + axis_class(j, ny) * 3;
+            const T *iv = tabT(ts) + JOFF + axis_class(j, ny) * 3;
             V4<T> rv;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
@@ -593,7 +639,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         };
         auto form = [&](const Unit &U, int m, int ts, unsigned char *stg, unsigned char *rp) {
             const T *rs = reinterpret_cast<const T *>(stg);
-            const T *itab = tabT(ts) + 243;
+            const T *itab = tabT(ts) + JOFF;
             const T *ps = reinterpret_cast<const T *>(stg + L::ARR);
             T *dst = reinterpret_cast<T *>(rp);
             const bool own_plane = m >= U.k0 && m < U.k1;
@@ -727,7 +773,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
 #pragma unroll
                 for (int h = 0; h < 3; ++h) {
                     const int jr = j - 1 + h;
-                    const float *irow = tb + 243 + axis_class(jr, ny) * 3;
+                    const float *irow = tb + JOFF + axis_class(jr, ny) * 3;
                     const int o = (w + h) * WX + HX + 4 * lane;
                     const V4<T> rv = ld4(rs + o);
                     V4<T> po = {{T(0), T(0), T(0), T(0)}};
@@ -932,11 +978,14 @@ __global__ void k_zinv(mb_stencil_dev st, double *inv64, float *inv32, float *pt
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < np; e += gridDim.x * blockDim.x) {
         const int k = e / PTAB, q = e - k * PTAB;
         float v = 0.0f;
-        if (q < 243) {
-            const size_t src = (size_t)k * 243 + q;
-            v = st.table32 ? st.table32[src] : (float)st.table[src];
-        } else if (q < 252) {
-            const size_t src = ((size_t)k * 9 + (q - 243)) * 27 + 13;
+        if (q < JOFF) {
+            const int row = q / CROW, col = q - row * CROW;
+            if (col < 27) {
+                const size_t src = (size_t)k * 243 + row * 27 + col;
+                v = st.table32 ? st.table32[src] : (float)st.table[src];
+            }
+        } else if (q < JOFF + 9) {
+            const size_t src = ((size_t)k * 9 + (q - JOFF)) * 27 + 13;
             v = 1.0f / (st.table32 ? st.table32[src] : (float)st.table[src]);
         }
         ptab32[e] = v;
