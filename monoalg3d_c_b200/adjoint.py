@@ -29,16 +29,19 @@ class Adjoint:
     sigma_cell: conductivity per cell (mS/um, grid order); gkr: gKr scaling per
     cell; sensors: grid indices; samples after every ``sample_every`` steps.
     Other keywords go to the tissue description (dt_pde, stims, cg_tolerance,
-    ...); the model is ten Tusscher 2006 in FP64.
+    ...); the model is ten Tusscher 2006.  precision "mixed" runs the forward
+    in the mixed form (FP32 cell model and CG recurrences) and its adjoint
+    with the cell model's Jacobian in FP32, every adjoint vector and gradient
+    accumulated in FP64.
     """
 
     def __init__(self, nx: int, ny: int, nz: int, sigma_cell: np.ndarray, gkr: np.ndarray, sensors: Sequence[int],
-                 nsteps: int, sample_every: int, checkpoint_every: int = 50, **kw):
+                 nsteps: int, sample_every: int, checkpoint_every: int = 50, precision: str = "fp64", **kw):
         self.n = nx * ny * nz
         self.ns = len(sensors)
         self.nsamples = nsteps // sample_every
         scale = self.scales(gkr)
-        d, keep = build_desc(nx, ny, nz, model="tt2006", precision="fp64", assembly="per_cell",
+        d, keep = build_desc(nx, ny, nz, model="tt2006", precision=precision, assembly="per_cell",
                              sigma_cell=np.asarray(sigma_cell, dtype=np.float64), current_scale=scale, **kw)
         sens = np.ascontiguousarray(sensors, dtype=np.int64)
         h = C.c_void_p()

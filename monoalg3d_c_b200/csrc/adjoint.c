@@ -1,7 +1,11 @@
 /* Discrete adjoint of the monodomain loop (host, C): gradients of a misfit
  * between simulated and observed V at sensor cells with respect to the
- * per-cell conductivity and the per-cell gKr scaling (ten Tusscher 2006, FP64,
- * per-cell conductivity, one Rush-Larsen sub-step per loop step).
+ * per-cell conductivity and the per-cell gKr scaling (ten Tusscher 2006,
+ * per-cell conductivity, one Rush-Larsen sub-step per loop step), for the
+ * FP64 forward or the mixed one (FP32 cell model and CG recurrences, FP64
+ * V and concentrations): the mixed adjoint forms the cell model's Jacobian in
+ * FP32, solves the transposed system with the mixed CG and accumulates every
+ * adjoint vector and gradient in FP64.
  *
  * Forward: from the tissue's initial state, run nsteps loop steps, sampling V
  * at the sensor cells after every sample_every steps and storing a snapshot of
@@ -25,6 +29,9 @@
 int mbk_adj_tt2006(const mb_ode_dev *o, const mb_ctrl *ctrl_n, const double *v_n, const double *sv_n,
                    const double *w, double alpha, const double *mu_in, double *mu_out, double *lam_out,
                    double *gth, cudaStream_t s);
+int mbk_adj_tt2006_mixed(const mb_ode_dev *o, const mb_ctrl *ctrl_n, const double *v_n, const double *sv64_n,
+                         const float *sv32_n, const double *w, double alpha, const double *mu_in, double *mu_out,
+                         double *lam_out, double *gth, cudaStream_t s);
 int mbk_adj_face_grad(const mb_stencil_dev *st, const double *sigma, const double *w, const double *v,
                       double mx, double my, double mz, double *gsig, cudaStream_t s);
 int mbk_adj_gather(const double *v, const int64_t *cells, int ns, double *out, cudaStream_t s);
@@ -71,9 +78,9 @@ int mb_adjoint_create(mb_adjoint **out, const mb_monodomain_desc *d, int nsteps,
                       int n_sensors, const int64_t *sensor_cells, int sample_every) {
     if (!out || !d || nsteps <= 0 || checkpoint_every <= 0 || n_sensors <= 0 || !sensor_cells || sample_every <= 0)
         return AERR(MB_ERR_ARG, "mb_adjoint_create: bad arguments");
-    if (d->model != MB_MODEL_TT2006 || d->precision != MB_PREC_FP64 || d->assembly != MB_ASSEMBLY_PER_CELL_SIGMA ||
-        !d->sigma_cell || !d->current_scale || d->dt_ode != d->dt_pde)
-        return AERR(MB_ERR_UNSUPPORTED, "the adjoint needs TT2006, FP64, per-cell sigma, conductance scalings and "
+    if (d->model != MB_MODEL_TT2006 || d->assembly != MB_ASSEMBLY_PER_CELL_SIGMA || !d->sigma_cell ||
+        !d->current_scale || d->dt_ode != d->dt_pde)
+        return AERR(MB_ERR_UNSUPPORTED, "the adjoint needs TT2006, per-cell sigma, conductance scalings and "
                                         "one ODE sub-step per loop step");
     const int64_t n = (int64_t)d->nx * d->ny * d->nz;
     for (int i = 0; i < n_sensors; ++i)
@@ -203,8 +210,9 @@ int mb_adjoint_backward(mb_adjoint *a, const double *dtraces, double *grad_sigma
             }
             double *v1, *v0, *sv0;
             mb_ctrl *c0;
+            void *snap0 = a->d_seg + a->snap * (size_t)k;
             mb_tissue_snapshot_parts(m, a->d_seg + a->snap * (size_t)(k + 1), &v1, NULL, NULL);
-            mb_tissue_snapshot_parts(m, a->d_seg + a->snap * (size_t)k, &v0, &sv0, &c0);
+            mb_tissue_snapshot_parts(m, snap0, &v0, &sv0, &c0);
             /* A w = lambda_{step+1} (warm start from the previous w) */
             AKK(mbk_adj_tol(a->d_lam, n, 1e-24, a->d_actrl, s));
             AKK(mbk_fcg_launch(&q, s));
@@ -212,7 +220,11 @@ int mb_adjoint_backward(mb_adjoint *a, const double *dtraces, double *grad_sigma
             AKK(mbk_adj_face_grad(&m->st, a->d_sigma, a->d_w, v1, a->mx, a->my, a->mz, a->d_gsig, s));
             /* through the Rush-Larsen step at (v_step, s_step) */
             ACK(cudaMemsetAsync(a->d_lam2, 0, nb, s));
-            AKK(mbk_adj_tt2006(&o, c0, v0, sv0, a->d_w, a->alpha, a->d_mu, a->d_mu2, a->d_lam2, a->d_gth, s));
+            if (m->desc.precision == MB_PREC_MIXED)
+                AKK(mbk_adj_tt2006_mixed(&o, c0, v0, sv0, mb_tissue_snapshot_sv32(m, snap0), a->d_w, a->alpha,
+                                         a->d_mu, a->d_mu2, a->d_lam2, a->d_gth, s));
+            else
+                AKK(mbk_adj_tt2006(&o, c0, v0, sv0, a->d_w, a->alpha, a->d_mu, a->d_mu2, a->d_lam2, a->d_gth, s));
             double *t = a->d_lam; a->d_lam = a->d_lam2; a->d_lam2 = t;
             t = a->d_mu; a->d_mu = a->d_mu2; a->d_mu2 = t;
             q.b = a->d_lam;

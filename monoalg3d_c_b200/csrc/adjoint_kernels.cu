@@ -22,24 +22,25 @@ MB_NS_BEGIN
 
 // ---- dual numbers ---------------------------------------------------------------
 
-template <int K>
+// value type T: double for the FP64 forward, float for the mixed one
+template <int K, typename T = double>
 struct Dual {
-    double v;
-    double d[K];
+    T v;
+    T d[K];
     __device__ __forceinline__ Dual() {}
-    __device__ __forceinline__ Dual(double x) : v(x) {
+    __device__ __forceinline__ Dual(double x) : v((T)x) {
 #pragma unroll
-        for (int k = 0; k < K; ++k) d[k] = 0.0;
+        for (int k = 0; k < K; ++k) d[k] = T(0);
     }
 };
 
-#define MB_DUAL_BIN(OP, VAL, DER)                                                            \
-    template <int K>                                                                         \
-    __device__ __forceinline__ Dual<K> operator OP(const Dual<K> &a, const Dual<K> &b) {     \
-        Dual<K> r;                                                                           \
-        r.v = VAL;                                                                           \
-        _Pragma("unroll") for (int k = 0; k < K; ++k) r.d[k] = DER;                          \
-        return r;                                                                            \
+#define MB_DUAL_BIN(OP, VAL, DER)                                                                      \
+    template <int K, typename T>                                                                       \
+    __device__ __forceinline__ Dual<K, T> operator OP(const Dual<K, T> &a, const Dual<K, T> &b) {      \
+        Dual<K, T> r;                                                                                  \
+        r.v = VAL;                                                                                     \
+        _Pragma("unroll") for (int k = 0; k < K; ++k) r.d[k] = DER;                                    \
+        return r;                                                                                      \
     }
 MB_DUAL_BIN(+, a.v + b.v, a.d[k] + b.d[k])
 MB_DUAL_BIN(-, a.v - b.v, a.d[k] - b.d[k])
@@ -47,38 +48,45 @@ MB_DUAL_BIN(*, a.v * b.v, a.d[k] * b.v + a.v * b.d[k])
 MB_DUAL_BIN(/, a.v / b.v, (a.d[k] * b.v - a.v * b.d[k]) / (b.v * b.v))
 #undef MB_DUAL_BIN
 
-template <int K>
-__device__ __forceinline__ Dual<K> operator-(const Dual<K> &a) {
-    Dual<K> r;
+template <int K, typename T>
+__device__ __forceinline__ Dual<K, T> operator-(const Dual<K, T> &a) {
+    Dual<K, T> r;
     r.v = -a.v;
 #pragma unroll
     for (int k = 0; k < K; ++k) r.d[k] = -a.d[k];
     return r;
 }
-template <int K> __device__ __forceinline__ bool operator<(const Dual<K> &a, const Dual<K> &b) { return a.v < b.v; }
-template <int K> __device__ __forceinline__ bool operator>(const Dual<K> &a, const Dual<K> &b) { return a.v > b.v; }
-template <int K> __device__ __forceinline__ bool operator<=(const Dual<K> &a, const Dual<K> &b) { return a.v <= b.v; }
-template <int K> __device__ __forceinline__ bool operator>=(const Dual<K> &a, const Dual<K> &b) { return a.v >= b.v; }
+template <int K, typename T>
+__device__ __forceinline__ bool operator<(const Dual<K, T> &a, const Dual<K, T> &b) { return a.v < b.v; }
+template <int K, typename T>
+__device__ __forceinline__ bool operator>(const Dual<K, T> &a, const Dual<K, T> &b) { return a.v > b.v; }
+template <int K, typename T>
+__device__ __forceinline__ bool operator<=(const Dual<K, T> &a, const Dual<K, T> &b) { return a.v <= b.v; }
+template <int K, typename T>
+__device__ __forceinline__ bool operator>=(const Dual<K, T> &a, const Dual<K, T> &b) { return a.v >= b.v; }
 
-template <int K>
-__device__ __forceinline__ Dual<K> chain(const Dual<K> &a, double val, double der) {
-    Dual<K> r;
+template <int K, typename T>
+__device__ __forceinline__ Dual<K, T> chain(const Dual<K, T> &a, T val, T der) {
+    Dual<K, T> r;
     r.v = val;
 #pragma unroll
     for (int k = 0; k < K; ++k) r.d[k] = der * a.d[k];
     return r;
 }
-template <int K> __device__ __forceinline__ Dual<K> mexp(const Dual<K> &a) {
-    const double e = exp(a.v);
+// the value-type functions mexp / mexpm1 / mlog / msqrt of mb_math.cuh
+template <int K, typename T> __device__ __forceinline__ Dual<K, T> mexp(const Dual<K, T> &a) {
+    const T e = mexp(a.v);
     return chain(a, e, e);
 }
-template <int K> __device__ __forceinline__ Dual<K> mexpm1(const Dual<K> &a) {
-    return chain(a, expm1(a.v), exp(a.v));
+template <int K, typename T> __device__ __forceinline__ Dual<K, T> mexpm1(const Dual<K, T> &a) {
+    return chain(a, mexpm1(a.v), mexp(a.v));
 }
-template <int K> __device__ __forceinline__ Dual<K> mlog(const Dual<K> &a) { return chain(a, log(a.v), 1.0 / a.v); }
-template <int K> __device__ __forceinline__ Dual<K> msqrt(const Dual<K> &a) {
-    const double s = sqrt(a.v);
-    return chain(a, s, 0.5 / s);
+template <int K, typename T> __device__ __forceinline__ Dual<K, T> mlog(const Dual<K, T> &a) {
+    return chain(a, mlog(a.v), T(1) / a.v);
+}
+template <int K, typename T> __device__ __forceinline__ Dual<K, T> msqrt(const Dual<K, T> &a) {
+    const T s = msqrt(a.v);
+    return chain(a, s, T(0.5) / s);
 }
 
 // ---- ODE adjoint ----------------------------------------------------------------
@@ -88,11 +96,13 @@ constexpr int ADJ_IN = TT_NEQ + 1;      // the 19 states and the gKr scaling
 
 // Column block [j0, j0 + K) of J_Phi, contracted with g: res[j] += sum_i g_i
 // d(out_i)/d(in_j).  Inputs 0..18 are the states (0 = V), input 19 the gKr
-// scaling.
-template <int K>
-__device__ __forceinline__ void adj_block(int j0, const double (&y)[TT_NEQ], const TTScale<double> &sc, double stim,
-                                          double dt, const double (&g)[TT_NEQ], double (&res)[ADJ_IN]) {
-    using D = Dual<K>;
+// scaling.  T: the arithmetic of the forward step (double; float for the
+// mixed form, whose right-hand side is FP32); the contraction with g and the
+// results are FP64.
+template <int K, typename T = double>
+__device__ __forceinline__ void adj_block(int j0, const T (&y)[TT_NEQ], const TTScale<T> &sc, T stim, T dt,
+                                          const double (&g)[TT_NEQ], double (&res)[ADJ_IN]) {
+    using D = Dual<K, T>;
     D yd[TT_NEQ];
 #pragma unroll
     for (int s = 0; s < TT_NEQ; ++s) {
@@ -127,7 +137,7 @@ __device__ __forceinline__ void adj_block(int j0, const double (&y)[TT_NEQ], con
         if (j0 + k >= ADJ_IN) break;
         double acc = 0.0;
 #pragma unroll
-        for (int i = 0; i < TT_NEQ; ++i) acc += g[i] * out[i].d[k];
+        for (int i = 0; i < TT_NEQ; ++i) acc += g[i] * (double)out[i].d[k];
         res[j0 + k] = acc;
     }
 }
@@ -157,6 +167,46 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_tt2006(mb_ode_dev o, const 
     const TTScale<double> sc = load_tt_scale<double>(o, t);
     double res[ADJ_IN];
     for (int j0 = 0; j0 < ADJ_IN; j0 += K) adj_block<K>(j0, y, sc, stim, o.dt, gi, res);
+    lam_out[g] = res[0];
+#pragma unroll
+    for (int s = 1; s < TT_NEQ; ++s) mu_out[s * ld + t] = res[s];
+    gth[t] += res[TT_NEQ];
+}
+
+// The same for the mixed forward (k_tt2006_mixed): the state from the mixed
+// rows of the snapshot (FP64 rows 1..5 = Ca_i, Ca_SR, Ca_ss, Na_i, K_i; FP32
+// rows 0..11 = the gates, row 12 = R'), the Jacobian in FP32 dual numbers
+// through the same model code, contracted and accumulated in FP64.
+template <int K>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_tt2006_mixed(mb_ode_dev o, const mb_ctrl *__restrict__ ctrl_n,
+                                                                  const double *__restrict__ v_n,
+                                                                  const double *__restrict__ sv64_n,
+                                                                  const float *__restrict__ sv32_n,
+                                                                  const double *__restrict__ w, double alpha,
+                                                                  const double *__restrict__ mu_in, double *mu_out,
+                                                                  double *lam_out, double *gth) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= o.n) return;
+    const uint32_t g = o.cell ? o.cell[t] : t;
+    const size_t ld = o.ld;
+    float y[TT_NEQ];
+    double gi[TT_NEQ];
+    y[TT_V] = (float)v_n[g];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) y[1 + k] = sv32_n[k * ld + t];
+    y[TT_CAI] = (float)sv64_n[1 * ld + t];
+    y[TT_CASR] = (float)sv64_n[2 * ld + t];
+    y[TT_CASS] = (float)sv64_n[3 * ld + t];
+    y[TT_NAI] = (float)sv64_n[4 * ld + t];
+    y[TT_KI] = (float)sv64_n[5 * ld + t];
+    y[TT_RPRIME] = sv32_n[12 * ld + t];
+    gi[0] = alpha * w[g];
+#pragma unroll
+    for (int s = 1; s < TT_NEQ; ++s) gi[s] = mu_in[s * ld + t];
+    const float stim = (float)cell_stim(o, ctrl_n, t);
+    const TTScale<float> sc = load_tt_scale<float>(o, t);
+    double res[ADJ_IN];
+    for (int j0 = 0; j0 < ADJ_IN; j0 += K) adj_block<K, float>(j0, y, sc, stim, (float)o.dt, gi, res);
     lam_out[g] = res[0];
 #pragma unroll
     for (int s = 1; s < TT_NEQ; ++s) mu_out[s * ld + t] = res[s];
@@ -232,6 +282,15 @@ extern "C" int mbk_adj_tt2006(const mb_ode_dev *o, const mb_ctrl *ctrl_n, const 
                               double *gth, cudaStream_t s) {
     const unsigned blocks = (o->n + ADJ_THREADS - 1) / ADJ_THREADS;
     k_adj_tt2006<2><<<blocks, ADJ_THREADS, 0, s>>>(*o, ctrl_n, v_n, sv_n, w, alpha, mu_in, mu_out, lam_out, gth);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int mbk_adj_tt2006_mixed(const mb_ode_dev *o, const mb_ctrl *ctrl_n, const double *v_n,
+                                    const double *sv64_n, const float *sv32_n, const double *w, double alpha,
+                                    const double *mu_in, double *mu_out, double *lam_out, double *gth, cudaStream_t s) {
+    const unsigned blocks = (o->n + ADJ_THREADS - 1) / ADJ_THREADS;
+    k_adj_tt2006_mixed<2><<<blocks, ADJ_THREADS, 0, s>>>(*o, ctrl_n, v_n, sv64_n, sv32_n, w, alpha, mu_in, mu_out,
+                                                        lam_out, gth);
     return (int)cudaGetLastError();
 }
 

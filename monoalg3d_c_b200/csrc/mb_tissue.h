@@ -86,6 +86,8 @@ size_t mb_tissue_snapshot_bytes(const mb_monodomain *m);
 int mb_tissue_snapshot(mb_monodomain *m, void *dev, int restore);
 /* Pointers into a snapshot: V, the FP64 state rows, the control block. */
 void mb_tissue_snapshot_parts(const mb_monodomain *m, void *dev, double **v, double **sv64, mb_ctrl **ctrl);
+/* The FP32 state rows of a snapshot (mixed precision; NULL otherwise). */
+float *mb_tissue_snapshot_sv32(const mb_monodomain *m, void *dev);
 /* New per-cell conductivity (grid order; PER_CELL_SIGMA tissues) and new
  * conductance scalings (MB_NUM_SCALES x grid; tissues created with them). */
 int mb_tissue_set_sigma(mb_monodomain *m, const double *sigma_cell);

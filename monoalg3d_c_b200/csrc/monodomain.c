@@ -1723,6 +1723,12 @@ void mb_tissue_snapshot_parts(const mb_monodomain *m, void *dev, double **v, dou
     if (ctrl) *ctrl = (mb_ctrl *)((char *)dev + off[4]);
 }
 
+float *mb_tissue_snapshot_sv32(const mb_monodomain *m, void *dev) {
+    size_t off[5], len[5];
+    snapshot_layout(m, off, len);
+    return len[3] ? (float *)((char *)dev + off[3]) : NULL;
+}
+
 int mb_tissue_set_sigma(mb_monodomain *m, const double *sigma_cell) {
     if (!m || !sigma_cell || m->desc.assembly != MB_ASSEMBLY_PER_CELL_SIGMA || !m->d_fx)
         return set_err(MB_ERR_ARG, "new conductivities need a per-cell-sigma tissue");

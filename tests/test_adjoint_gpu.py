@@ -148,3 +148,38 @@ def test_autograd_function():
     np.testing.assert_allclose(k.grad.numpy(), gk, rtol=1e-12, atol=0)
     assert np.abs(gs).max() > 0 and np.abs(gk).max() > 0
     adj.close()
+
+
+def test_mixed_forward_adjoint():
+    """The configuration's form: FP32 forward (mixed cell model and CG), FP64
+    accumulation of the adjoint and the gradients.  Its directional
+    derivatives against the FP64 adjoint's at the same point (1e-3 relative:
+    the Jacobian is formed in FP32) and against central differences of the
+    mixed loop itself (1e-2: the FP32 forward's rounding limits how small the
+    difference step can be, 1e-2 relative in sigma)."""
+    from monoalg3d_c_b200.adjoint import Adjoint
+    nx, ny, steps, sigma, gkr, sensors = _problem()
+    a64 = Adjoint(nx, ny, 1, sigma, gkr, sensors, nsteps=steps, sample_every=50, checkpoint_every=50, **_kw())
+    am = Adjoint(nx, ny, 1, sigma, gkr, sensors, nsteps=steps, sample_every=50, checkpoint_every=50,
+                 precision="mixed", **_kw())
+    target = a64.forward(sigma * 1.2, gkr * 0.9)
+    loss = lambda t: 0.5 * np.sum((t - target) ** 2)  # noqa: E731
+    t64 = a64.forward(sigma, gkr)
+    g64s, g64k = a64.backward(t64 - target)
+    tm = am.forward(sigma, gkr)
+    gms, gmk = am.backward(tm - target)
+    rng = np.random.default_rng(11)
+    for trial in range(3):
+        d = rng.standard_normal(sigma.size)
+        dm, d64 = float(np.sum(gms * sigma * d)), float(np.sum(g64s * sigma * d))
+        h = 1e-2
+        fd = (loss(am.forward(sigma * (1 + h * d), gkr)) - loss(am.forward(sigma * (1 - h * d), gkr))) / (2 * h)
+        print(f"sigma direction {trial}: mixed adjoint {dm:.6e}, FP64 adjoint {d64:.6e}, mixed FD {fd:.6e}")
+        assert abs(dm - d64) <= 1e-3 * abs(d64)
+        assert abs(dm - fd) <= 1e-2 * abs(fd)
+        dk = rng.standard_normal(sigma.size)
+        km, k64 = float(np.sum(gmk * dk)), float(np.sum(g64k * dk))
+        print(f"gKr direction {trial}: mixed adjoint {km:.6e}, FP64 adjoint {k64:.6e}")
+        assert abs(km - k64) <= 1e-3 * abs(k64)
+    a64.close()
+    am.close()
