@@ -175,8 +175,8 @@ class ClockSampler:
 #   dram__bytes_write.sum) per active cell and CG iteration of one launch
 PROFILED_CG_TRAFFIC = {
     # k_zcg<1, 8, 3, 2> on the 0.72-scale slab (360x360x72, every vector
-    # larger than L2): 6.411 GB over 9.33 M cells x 15 iterations
-    ("slab_500x500x100_torord_rotating_fibres", 301): 45.8,
+    # larger than L2): 6.445 GB over 9.33 M cells x 15 iterations
+    ("slab_500x500x100_torord_rotating_fibres", 301): 46.0,
 }
 #   (workload, "mixed" | "fp64", ode variant) -> pipe utilisation and MUFU
 #   (XU pipe) warp instructions x 32 per cell-step of one launch
