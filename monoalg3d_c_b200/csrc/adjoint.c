@@ -186,6 +186,9 @@ int mb_adjoint_backward(mb_adjoint *a, const double *dtraces, double *grad_sigma
         ACK(cudaMemcpy(a->d_actrl, &c, sizeof c, cudaMemcpyHostToDevice));
     }
     mb_pcg_dev q = m->pcg;
+    /* the z-march kernel's tensor maps address the tissue's own vectors (the
+     * per-cell operator of the adjoint never selects it) */
+    if (q.form == MB_PCG_ZMARCH) return AERR(MB_ERR_UNSUPPORTED, "the adjoint's transposed solve on the z-march CG");
     q.ctrl = a->d_actrl;
     q.x = a->d_w;
     q.b = a->d_lam;

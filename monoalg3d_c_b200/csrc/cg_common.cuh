@@ -20,9 +20,10 @@ struct Args {
     float *r32, *pa32, *pb32, *z32;
     double *ap64;              // A p of the current direction (stored by Q, read by U)
     float *ap32;
+    float *ap32b;              // the z-march fused pass's second A p buffer
     const double *inv_diag64;  // Jacobi 1/diag per cell (FP64 form)
     const float *inv_diag32;   // Jacobi 1/diag per cell (mixed form)
-    double *partials;          // 2 x 4 x gridDim.x partials
+    double *partials;          // 2 x 8 x gridDim.x partials
     mb_ctrl *ctrl;
     unsigned *bar;             // [0] arrivals since launch (zeroed before each launch)
     int *status;
@@ -40,11 +41,14 @@ struct Args {
 // returns false (the caller leaves the kernel).
 template <int NV, int NT>
 __device__ __forceinline__ bool grid_reduce(const Args &a, double (&v)[NV], double (&out)[NV], int &red) {
+    static_assert(NV >= 1 && NV <= 8, "the partials hold up to 8 values per block");
+    // partials loaded per lane before the adds (fewer for many values)
+    constexpr int J = NV <= 4 ? 8 : 4;
     __shared__ double sm[NV][NT / 32];
     __shared__ double tot[NV];
     __shared__ int flag;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double *part = a.partials + (size_t)(red & 1) * 4 * gridDim.x;
+    double *part = a.partials + (size_t)(red & 1) * 8 * gridDim.x;
     const unsigned target = (unsigned)(red + 1) * gridDim.x;
     red++;
 #pragma unroll
@@ -81,24 +85,24 @@ __device__ __forceinline__ bool grid_reduce(const Args &a, double (&v)[NV], doub
         // arrivals lane 0 observed
         cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
         if (ok) {
-            // every partial of a chunk of up to 256 blocks is loaded before any
-            // is added, so the reads cost one L2 round trip, not one per value
+            // every partial of a chunk of up to 32 J blocks is loaded before
+            // any is added, so the reads cost one L2 round trip, not one per value
             double s[NV];
 #pragma unroll
             for (int q = 0; q < NV; ++q) s[q] = 0.0;
-            for (unsigned base = 0; base < gridDim.x; base += 256) {
-                double vals[NV][8];
+            for (unsigned base = 0; base < gridDim.x; base += 32 * J) {
+                double vals[NV][J];
 #pragma unroll
                 for (int q = 0; q < NV; ++q)
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
+                    for (int j = 0; j < J; ++j) {
                         const unsigned bk = base + lane + 32 * j;
                         vals[q][j] = bk < gridDim.x ? __ldcg(&part[(size_t)q * gridDim.x + bk]) : 0.0;
                     }
 #pragma unroll
                 for (int q = 0; q < NV; ++q)
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) s[q] += vals[q][j];
+                    for (int j = 0; j < J; ++j) s[q] += vals[q][j];
             }
 #pragma unroll
             for (int q = 0; q < NV; ++q) {

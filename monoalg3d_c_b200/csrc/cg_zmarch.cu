@@ -44,6 +44,7 @@
 // still in flight and leave the kernel; the other blocks then time out at
 // their next grid reduction and leave too.
 #include <cuda.h>
+#include <cstring>
 #include "cg_common.cuh"
 
 namespace mb {
@@ -57,6 +58,7 @@ constexpr int TX = 128;            // tile width in x: 32 lanes x 4 cells
 constexpr int HX = 4;              // x halo per side (16 bytes of FP32)
 constexpr int WX = TX + 2 * HX;    // staged row length
 constexpr int RING = 4;            // ring planes
+constexpr int MAPS = 8;            // tensor maps per variant
 
 // Division by a fixed divisor d as a multiply and shifts (Granlund and
 // Montgomery, "Division by invariant integers using multiplication", 1994,
@@ -98,16 +100,27 @@ constexpr int TSLOT = JOFF + 12;   // entries per plane slot (a multiple of 4)
 constexpr int PTAB = TSLOT;        // the same block in global memory (FP32, 16-byte multiple)
 constexpr int QDLY = 2;            // window Q pass: the stage of entry e is refilled at step e + QDLY
 
-template <typename T, int W, int S, bool QW = false>
+// Iteration forms (the kernel's MODE): the ring Q pass and the U pass; the
+// window Q pass and the U pass; the fused pass (mixed only: one stencil pass
+// and one reduction per iteration).
+enum { QRING = 0, QWIN = 1, FUSED = 2 };
+
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+template <typename T, int W, int S, int MODE = QRING>
 struct Lay {
     static constexpr int H = W + 2;                         // staged rows
     static constexpr int ELEMS = H * WX;                    // one staged plane
     static constexpr int ARR = r128(ELEMS * (int)sizeof(T));
+    static constexpr int XARR = r128(ELEMS * 8);            // a staged plane of doubles (x)
     // window Q pass: r, p_old and the plane's table (FP32) per stage
-    static constexpr int QSTAGE = (QW && sizeof(T) == 4) ? 2 * ARR + r128(PTAB * 4) : 0;
-    static constexpr int STAGE0 = 2 * ARR > r128(ELEMS * 8) ? 2 * ARR : r128(ELEMS * 8);
-    static constexpr int STAGE = QSTAGE > STAGE0 ? QSTAGE : STAGE0;
-    static constexpr int RPLANE = r128(ELEMS * 8);          // ring planes hold doubles (residual pass)
+    static constexpr int QSTAGE = (MODE == QWIN && sizeof(T) == 4) ? 2 * ARR + r128(PTAB * 4) : 0;
+    // fused pass: r, A p and p_old; its residual pass: x and p
+    static constexpr int FSTAGE = MODE == FUSED ? cmax(3 * ARR, XARR + ARR) : 0;
+    static constexpr int STAGE = cmax(cmax(2 * ARR, XARR), cmax(QSTAGE, FSTAGE));
+    // ring planes hold doubles (residual pass); in the fused pass a ring
+    // plane holds the direction p and then the residual r
+    static constexpr int RPLANE = MODE == FUSED ? cmax(XARR, 2 * ARR) : XARR;
     static constexpr int BARS = 128;
     // the coefficient rows and Jacobi values of up to four planes, both
     // precisions (the residual pass applies the FP64 rows)
@@ -294,6 +307,11 @@ __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, 
     if constexpr (sizeof(R) == 4) load_row(cm, cc);
     R acc[4] = {R(0), R(0), R(0), R(0)};
     const int off = HX + 4 * lane;
+    // the value beyond the tile's row: left of it for lane 0, right of it
+    // for the others (used by lane 31) -- two distinct addresses in
+    // different banks, one shared-memory wavefront per row (each lane
+    // reading its own neighbour would take four to eight)
+    const int hoff = lane == 0 ? HX - 1 : HX + TX;
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz) {
         const R *pl = dz < 0 ? lo : (dz == 0 ? mid : hi);
@@ -301,16 +319,17 @@ __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, 
         for (int dy = -1; dy <= 1; ++dy) {
             const unsigned rb = (mask >> ((dz + 1) * 9 + (dy + 1) * 3)) & 7u;
             if (!rb) continue;
-            const R *rowp = pl + (w + 1 + dy) * WX + off;
+            const R *rowb = pl + (w + 1 + dy) * WX;
+            const R *rowp = rowb + off;
             const V4<R> m4 = ld4(rowp);
+            const R he = rowb[hoff];
             const R sl = __shfl_up_sync(0xffffffffu, m4.v[3], 1);
             const R sr = __shfl_down_sync(0xffffffffu, m4.v[0], 1);
             R wv[6];
-            // the values beyond the tile's row (a select, not a branch: a
-            // branch per row keeps the compiler from scheduling the rows'
-            // loads ahead, measured slower)
-            wv[0] = lane == 0 ? rowp[-1] : sl;
-            wv[5] = lane == 31 ? rowp[4] : sr;
+            // (selects, not a branch: a branch per row keeps the compiler
+            // from scheduling the rows' loads ahead, measured slower)
+            wv[0] = lane == 0 ? he : sl;
+            wv[5] = lane == 31 ? he : sr;
 #pragma unroll
             for (int c = 0; c < 4; ++c) wv[c + 1] = m4.v[c];
 #pragma unroll
@@ -527,10 +546,11 @@ struct Tabs {
 
 // ---- the solve ----------------------------------------------------------------
 
-template <bool MIXED, int W, int S, int MINB, bool QW>
+template <bool MIXED, int W, int S, int MINB, int MODE>
 __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
     using T = typename Prec<MIXED>::T;
-    using L = Lay<T, W, S, QW>;
+    using L = Lay<T, W, S, MODE>;
+    static_assert(MODE != FUSED || MIXED, "the fused pass is the mixed form's");
     static_assert(S <= 4, "the barrier area holds 4 + 4 + 4 mbarriers");
     // Dynamic shared memory starts after the static reduction arrays of
     // grid_reduce, at an offset aligned to 16 bytes only; it is declared
@@ -564,7 +584,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
     if (threadIdx.x == 0) {
         // the maps were written by a copy from the host: acquire them for the
         // tensor-map proxy before the first bulk copy reads them
-        for (int q = 0; q < 4; ++q)
+        for (int q = 0; q < (MODE == FUSED ? MAPS : 4); ++q)
             asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(z.maps + q) : "memory");
         for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
         // window Q pass: full (the copies of a stage) and empty (every warp
@@ -591,15 +611,29 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
     };
 
     // ---- residual pass: r = b - A x (FP64), partials r.z, r.r, r64.r64 ----------
-    auto residual = [&](double (&acc)[3]) -> bool {
+    // With pk (the fused form's refinement) the stencil's input is x + alx pk,
+    // the update of x the fused form has not yet applied, formed from the
+    // staged x and pk in the same FP64 fma that later applies it to x.  The
+    // FP32 residual goes to rdst.
+    auto residual = [&](T *rdst, const T *pk, double alx, double (&acc)[3]) -> bool {
+        const CUtensorMap *mpk = pk == bufa ? tm_pa : tm_pb;
         auto issue = [&](const Unit &U, int m, unsigned char *stg, uint64_t *bar) {
-            mbar_expect_tx(bar, (unsigned)(L::ELEMS * 8));
+            mbar_expect_tx(bar, (unsigned)(L::ELEMS * 8) + (pk ? (unsigned)(L::ELEMS * sizeof(T)) : 0u));
             tma_load_3d(stg, tm_x, bar, U.x0 - HX, U.y0 - 1, m);
+            if (pk) tma_load_3d(stg + L::XARR, mpk, bar, U.x0 - HX, U.y0 - 1, m);
         };
         auto form = [&](const Unit &, int, int, unsigned char *stg, unsigned char *rp) {
             const double2 *src = reinterpret_cast<const double2 *>(stg);
             double2 *dst = reinterpret_cast<double2 *>(rp);
-            for (int e = threadIdx.x; e < L::ELEMS / 2; e += blockDim.x) dst[e] = src[e];
+            if (!pk) {
+                for (int e = threadIdx.x; e < L::ELEMS / 2; e += blockDim.x) dst[e] = src[e];
+            } else {
+                const T *ps = reinterpret_cast<const T *>(stg + L::XARR);
+                for (int e = threadIdx.x; e < L::ELEMS / 2; e += blockDim.x) {
+                    const double2 xv = src[e];
+                    dst[e] = make_double2(fma(alx, (double)ps[2 * e], xv.x), fma(alx, (double)ps[2 * e + 1], xv.y));
+                }
+            }
         };
         auto out = [&](const Unit &U, int k, int ts, unsigned char *lo, unsigned char *mid, unsigned char *hi) {
             const int j = U.y0 + w, i0 = U.x0 + 4 * lane;
@@ -623,7 +657,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
                 acc[1] += (double)rt * (double)rt;
                 acc[2] += r64 * r64;
             }
-            st4(r + g0, rv);
+            st4(rdst + g0, rv);
         };
         return zpass<W, S>(z, a, smem, L::TABS, L::STAGE, L::RPLANE, pp, issue, tabs, form, out);
     };
@@ -687,7 +721,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         return zpass<W, S>(z, a, smem, L::TABS, L::STAGE, L::RPLANE, pp, issue, tabs, form, out);
     };
 
-    // ---- window Q pass (QW, mixed): the same products without the ring ----------
+    // ---- window Q pass (QWIN, mixed): the same products without the ring ----------
     // Each warp forms the direction p for its own row and the rows above and
     // below it (one row of four cells per lane) straight from the staged r
     // and p_old, keeps p of the last three planes in registers (win) and
@@ -895,8 +929,221 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         }
     };
 
+    // ---- fused pass (FUSED, mixed): one stencil pass per iteration -------------
+    // Iteration k forms, from the staged r_{k-1}, A p_{k-1} and p_{k-1} (halo
+    // included),
+    //   r_k = r_{k-1} - alpha_{k-1} A p_{k-1}   (the U pass's FP32 fma)
+    //   p_k = r_k / diag + beta_{k-1} p_{k-1}    (the Q pass's)
+    // into the ring (p, then r), stores the tile's cells of r_k and p_k,
+    // applies x += alx p_{k-1} to the tile's cells (FP64; x of the next plane
+    // is loaded one plane ahead), and sums q = A p_k into the partials
+    //   p.q, q.z, q.Mq, q.r, q.q, r.z, r.r     (z = M r_k, M = 1 / diag)
+    // One reduction then gives r_k.z_k and r_k.r_k of the stored r_k,
+    // alpha_k = r.z / p.q, and r_{k+1}.z_{k+1} and r_{k+1}.r_{k+1} as
+    //   r.z - 2 a q.z + a^2 q.Mq,   r.r - 2 a q.r + a^2 q.q
+    // with a = alpha_k rounded to FP32 (the value the FP32 update of r
+    // applies): exact up to the rounding of r_{k+1} itself (about 1e-7
+    // relative), which is all beta_k (p_{k+1} is formed before r_{k+1}.z_{k+1}
+    // can be summed) and the refinement test need; alpha_{k+1} then uses the
+    // stored r_{k+1}'s own sums, so no error accumulates.  r and A p
+    // alternate between two buffers, since other blocks read the halo of the
+    // ones this pass replaces.  first: r_k is the staged residual and
+    // p_k = M r_k (no A p staged); xupd: p_{k-1} is staged for the pending
+    // update of x.
+    // (selected, not indexed: a run-time index would put the pairs in local memory)
+    T *const rb0 = r, *const rb1 = MIXED ? (T *)a.z32 : r;
+    T *const ab0 = apb, *const ab1 = MIXED ? (T *)a.ap32b : apb;
+    auto rbuf = [&](int i) { return i ? rb1 : rb0; };
+    auto fpass = [&](bool first, bool xupd, double alx, int rsel, int asel, const T *pold, T *pw, double alpha,
+                     double beta, double (&d7)[7]) -> bool {
+        const CUtensorMap *mr = rsel ? z.maps + 4 : tm_r;
+        const CUtensorMap *ma = asel ? z.maps + 6 : z.maps + 5;
+        const CUtensorMap *mp = pold == bufa ? tm_pa : tm_pb;
+        T *rout = rsel ? rb0 : rb1;
+        T *aout = asel ? ab0 : ab1;
+        const T al = (T)alpha, bt = (T)beta;
+        const bool cont = !first;
+        const unsigned arrays = 1u + (cont ? 1u : 0u) + ((cont || xupd) ? 1u : 0u);
+        auto issue = [&](const Unit &U, int m, unsigned char *stg, uint64_t *bar) {
+            mbar_expect_tx(bar, (unsigned)(L::ELEMS * sizeof(T)) * arrays);
+            tma_load_3d(stg, mr, bar, U.x0 - HX, U.y0 - 1, m);
+            if (cont) tma_load_3d(stg + L::ARR, ma, bar, U.x0 - HX, U.y0 - 1, m);
+            if (cont || xupd) tma_load_3d(stg + 2 * L::ARR, mp, bar, U.x0 - HX, U.y0 - 1, m);
+        };
+        // the lane's four cells of tile row w (x of the plane being updated)
+        const int jw = w, xl = 4 * lane;
+        V4<double> xnext = {{0.0, 0.0, 0.0, 0.0}};
+        auto form = [&](const Unit &U, int m, int ts, unsigned char *stg, unsigned char *rp) {
+            const T *rs = reinterpret_cast<const T *>(stg);
+            const T *as = reinterpret_cast<const T *>(stg + L::ARR);
+            const T *ps = reinterpret_cast<const T *>(stg + 2 * L::ARR);
+            const T *itab = tabT(ts) + JOFF;
+            T *dp = reinterpret_cast<T *>(rp);
+            T *dr = reinterpret_cast<T *>(rp + L::ARR);
+            const bool own_plane = m >= U.k0 && m < U.k1;
+            constexpr int QX = WX / 4;
+            for (int e = threadIdx.x; e < L::H * QX; e += blockDim.x) {
+                const int h = e / QX, xq = e - h * QX;
+                const int o = h * WX + 4 * xq;
+                const int i = U.x0 - HX + 4 * xq, j = U.y0 - 1 + h;
+                V4<T> rk = ld4(rs + o);
+                V4<T> po = {{T(0), T(0), T(0), T(0)}};
+                if (cont) {
+                    const V4<T> av = ld4(as + o);
+                    po = ld4(ps + o);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) rk.v[q] = fma(-al, av.v[q], rk.v[q]);
+                }
+                const T *irow = itab + axis_class(j, ny) * 3;
+                T iv[4];
+                if (i > 0 && i + 3 < nx - 1) {
+                    iv[0] = iv[1] = iv[2] = iv[3] = irow[1];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) iv[q] = irow[axis_class(i + q, nx)];
+                }
+                V4<T> pv;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const T zz = pre ? mul_rn(iv[q], rk.v[q]) : rk.v[q];
+                    pv.v[q] = cont ? fma(bt, po.v[q], zz) : zz;
+                }
+                st4(dp + o, pv);
+                st4(dr + o, rk);
+                if (own_plane && h >= 1 && h <= W && xq >= HX / 4 && xq < (HX + TX) / 4 && i < nx && j < ny) {
+                    const size_t g = (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * m);
+                    st4(pw + g, pv);
+                    if (cont) st4(rout + g, rk);
+                }
+            }
+            if (!xupd) return;
+            const int j = U.y0 + jw, i0 = U.x0 + xl;
+            if (j >= ny || i0 >= nx) return;
+            if (own_plane) {
+                const V4<T> pk = ld4(ps + (jw + 1) * WX + HX + xl);
+                V4<double> xn;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) xn.v[q] = fma(alx, (double)pk.v[q], xnext.v[q]);
+                st4(a.x + (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * m), xn);
+            }
+            // x of the next plane of this unit, used by the next step's form
+            if (m + 1 >= U.k0 && m + 1 < U.k1)
+                xnext = ld4(a.x + (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * (m + 1)));
+        };
+        auto out = [&](const Unit &U, int k, int ts, unsigned char *lo, unsigned char *mid, unsigned char *hi) {
+            const int j = U.y0 + w, i0 = U.x0 + 4 * lane;
+            if (j >= ny) return;
+            const T *pm = reinterpret_cast<const T *>(mid);
+            const V4<T> q = apply27<T, W>(st, reinterpret_cast<const T *>(lo), pm, reinterpret_cast<const T *>(hi),
+                                          tabT(ts), i0, j, w, lane);
+            if (i0 >= nx) return;
+            const size_t g0 = (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * k);
+            st4(aout + g0, q);
+            const int oc = (w + 1) * WX + HX + 4 * lane;
+            const V4<T> pc = ld4(pm + oc);
+            const V4<T> rc = ld4(reinterpret_cast<const T *>(mid + L::ARR) + oc);
+            T iv[4] = {T(1), T(1), T(1), T(1)};
+            if (pre) {
+                const T *irow = tabT(ts) + JOFF + axis_class(j, ny) * 3;
+                iv[0] = i0 == 0 ? irow[0] : irow[1];
+                iv[1] = iv[2] = irow[1];
+                iv[3] = i0 + 3 == nx - 1 ? irow[2] : irow[1];
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const double qd = (double)q.v[e];
+                const T zz = pre ? mul_rn(iv[e], rc.v[e]) : rc.v[e];
+                const T mq = pre ? mul_rn(iv[e], q.v[e]) : q.v[e];
+                const double rd = (double)rc.v[e];
+                d7[0] += (double)pc.v[e] * qd;
+                d7[1] += qd * (double)zz;
+                d7[2] += qd * (double)mq;
+                d7[3] += qd * rd;
+                d7[4] += qd * qd;
+                d7[5] += rd * (double)zz;
+                d7[6] += rd * rd;
+            }
+        };
+        return zpass<W, S>(z, a, smem, L::TABS, L::STAGE, L::RPLANE, pp, issue, tabs, form, out);
+    };
+
+    if constexpr (MODE == FUSED) {
+        // The mixed loop of the other forms (same refinement rule and stop
+        // test), with one reduction per iteration.  x of the last direction
+        // is applied by the next fused pass, or by the residual pass's input
+        // and then the final sweep below.
+        double acc[3] = {0.0, 0.0, 0.0}, s3[3];
+        if (!residual(rbuf(0), nullptr, 0.0, acc)) return;
+        if (!grid_reduce<3, 32 * W>(a, acc, s3, red)) return;
+        double rz = s3[0], rr = s3[1];
+        double error = s3[2], rr_ref = s3[2];
+        int its = 1, refinements = 1;
+        bool done = !(s3[2] >= tol) || !(1 < max_its);
+        bool first = true, xupd = false;
+        double alpha = 0.0, beta = 0.0;
+        int rsel = 0, asel = 0;
+        T *pcur = bufb;
+        while (!done) {
+            T *pnew = pcur == bufa ? bufb : bufa;
+            double d7[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, s7[7];
+            if (!fpass(first, xupd, alpha, rsel, asel, pcur, pnew, alpha, beta, d7)) return;
+            if (!grid_reduce<7, 32 * W>(a, d7, s7, red)) return;
+            if (!first) rsel ^= 1;
+            asel ^= 1;
+            pcur = pnew;
+            rz = s7[5];
+            rr = s7[6];
+            alpha = (pre ? rz : rr) / s7[0];
+            const double af = (double)(T)alpha;
+            const double rz_n = rz - 2.0 * af * s7[1] + af * af * s7[2];
+            const double rr_n = rr - 2.0 * af * s7[3] + af * af * s7[4];
+            xupd = true;
+            its += 1;
+            if (rr_n <= fmax(c->refine_floor, ratio * rr_ref) || its >= max_its) {
+                double t3[3] = {0.0, 0.0, 0.0};
+                if (!residual(rbuf(rsel), pcur, alpha, t3)) return;
+                if (!grid_reduce<3, 32 * W>(a, t3, s3, red)) return;
+                refinements += 1;
+                error = s3[2];
+                rr_ref = s3[2];
+                rz = s3[0];
+                rr = s3[1];
+                first = true;
+                if (s3[2] <= tol || its >= max_its) done = true;
+            } else {
+                beta = pre ? rz_n / rz : rr_n / rr;
+                rz = rz_n;
+                rr = rr_n;
+                error = rr_n;
+                first = false;
+            }
+        }
+        if (xupd) {
+            // x += alpha p of the last direction; every block has finished the
+            // residual pass that read x (its reduction was a grid barrier)
+            const unsigned groups = (unsigned)(nx >> 2) * (unsigned)ny * (unsigned)nz;
+            for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+                const size_t g0 = (size_t)q << 2;
+                const V4<T> pv = ld4(pcur + g0);
+                V4<double> xv = ld4(a.x + g0);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) xv.v[e] = fma(alpha, (double)pv.v[e], xv.v[e]);
+                st4(a.x + g0, xv);
+            }
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            c->its = its;
+            c->error = error;
+            c->refinements = refinements;
+            c->rz = rz;
+            c->rr = rr;
+            c->done = 1;
+        }
+        return;
+    }
+
     double acc[3] = {0.0, 0.0, 0.0}, s3[3];
-    if (!residual(acc)) return;
+    if (!residual(r, nullptr, 0.0, acc)) return;
     if (!grid_reduce<3, 32 * W>(a, acc, s3, red)) return;
     double rz = s3[0], rr = s3[1];
     double error = s3[2], rr_ref = s3[2];
@@ -910,7 +1157,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         T *pnew = pcur == bufa ? bufb : bufa;
         double q1[1] = {0.0}, s1[1];
         bool qok;
-        if constexpr (QW && MIXED) qok = qpass_w(first, pcur, pnew, beta, q1[0]);
+        if constexpr (MODE == QWIN && MIXED) qok = qpass_w(first, pcur, pnew, beta, q1[0]);
         else qok = qpass(first, pcur, pnew, beta, q1[0]);
         if (!qok) return;
         if (!grid_reduce<1, 32 * W>(a, q1, s1, red)) return;
@@ -936,7 +1183,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
             if (s2[1] <= fmax(c->refine_floor, ratio * rr_ref) || its >= max_its) {
                 // FP64 true residual replaces the FP32 recurrence; restart from it
                 double t3[3] = {0.0, 0.0, 0.0};
-                if (!residual(t3)) return;
+                if (!residual(r, nullptr, 0.0, t3)) return;
                 if (!grid_reduce<3, 32 * W>(a, t3, s3, red)) return;
                 refinements += 1;
                 error = s3[2];
@@ -998,32 +1245,37 @@ struct Variant {
     const void *fn;
     int warps;     // tile rows W (threads = 32 W)
     int bytes;     // dynamic shared memory
+    int mode;      // QRING, QWIN or FUSED
 };
 
-template <bool MIXED, int W, int S, int MINB, bool QW = false>
+template <bool MIXED, int W, int S, int MINB, int MODE = QRING>
 constexpr Variant make() {
-    return {(const void *)k_zcg<MIXED, W, S, MINB, QW>, W, Lay<typename Prec<MIXED>::T, W, S, QW>::BYTES};
+    return {(const void *)k_zcg<MIXED, W, S, MINB, MODE>, W, Lay<typename Prec<MIXED>::T, W, S, MODE>::BYTES, MODE};
 }
 
-// Mixed: the last three run the window Q pass.  FP64 has no window pass;
-// its last three are ring-pass shapes whose shared memory fits (four stages
-// of FP64 planes of W = 16 do not).
-constexpr int NUM_VARIANTS = 7;
+// Mixed: 4-6 run the window Q pass, 7-9 the fused pass.  FP64 has neither
+// (its iterations keep the U pass, whose r.r decides the stop exactly as the
+// reference's loop does); its 4-6 are ring-pass shapes whose shared memory
+// fits (four stages of FP64 planes of W = 16 do not) and 7-9 are empty.
+constexpr int NUM_VARIANTS = 10;
 
 static Variant variant(int mixed, int v) {
     static const Variant t64[NUM_VARIANTS] = {make<false, 8, 3, 1>(),  make<false, 8, 3, 2>(),
                                               make<false, 16, 3, 1>(), make<false, 4, 3, 3>(),
                                               make<false, 8, 4, 2>(),  make<false, 16, 3, 1>(),
-                                              make<false, 4, 4, 3>()};
-    static const Variant t32[NUM_VARIANTS] = {make<true, 8, 3, 1>(),        make<true, 8, 3, 2>(),
-                                              make<true, 16, 3, 1>(),       make<true, 4, 3, 3>(),
-                                              make<true, 8, 4, 2, true>(),  make<true, 16, 4, 1, true>(),
-                                              make<true, 4, 4, 3, true>()};
+                                              make<false, 4, 4, 3>(),  Variant{nullptr, 0, 0, 0},
+                                              Variant{nullptr, 0, 0, 0},  Variant{nullptr, 0, 0, 0}};
+    static const Variant t32[NUM_VARIANTS] = {
+        make<true, 8, 3, 1>(),        make<true, 8, 3, 2>(),         make<true, 16, 3, 1>(),
+        make<true, 4, 3, 3>(),        make<true, 8, 4, 2, QWIN>(),   make<true, 16, 4, 1, QWIN>(),
+        make<true, 4, 4, 3, QWIN>(),  make<true, 8, 3, 2, FUSED>(),  make<true, 16, 3, 1, FUSED>(),
+        make<true, 4, 3, 3, FUSED>()};
     return mixed ? t32[v] : t64[v];
 }
 
 // Resident blocks of a variant per SM x SMs (0 where it does not fit).
 static int grid_of(const Variant &var) {
+    if (!var.fn) return 0;
     int dev = 0, sms = 0, per = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
@@ -1115,21 +1367,34 @@ extern "C" int mbk_zcg_inv_tables(const mb_stencil_dev *st, double *inv64, float
 
 extern "C" int mbk_zcg_ptab_floats(void) { return PTAB; }
 
-// Tensor maps of every variant (4 per variant: r, p buffer a, p buffer b,
-// x), encoded on the host and copied to a device array p->zc_maps allocated
-// here (freed by the tissue).  Called once the CG buffers exist, before any
+// Tensor maps of every variant (MAPS per variant: r, p buffer a, p buffer b,
+// x, and for the fused pass the second r buffer and both A p buffers),
+// encoded on the host and copied to a device array p->zc_maps allocated here
+// (freed by the tissue).  Called once the CG buffers exist, before any
 // launch or stream capture.  Returns 0 or a CUDA error code.
 extern "C" int mbk_zcg_prepare(mb_pcg_dev *p) {
     const int nx = p->st.nx, ny = p->st.ny, nz = p->st.nz;
     const int elem = p->mixed ? 4 : 8;
-    alignas(64) CUtensorMap tm[NUM_VARIANTS * 4];
-    const void *bases[4] = {p->mixed ? (const void *)p->r32 : (const void *)p->r64,
-                            p->mixed ? (const void *)p->pa32 : (const void *)p->pa64,
-                            p->mixed ? (const void *)p->pb32 : (const void *)p->pb64, (const void *)p->x};
-    for (int v = 0; v < NUM_VARIANTS; ++v)
-        for (int q = 0; q < 4; ++q)
-            if (!encode(&tm[4 * v + q], bases[q], q == 3 ? 8 : elem, nx, ny, nz, variant(p->mixed, v).warps))
+    alignas(64) CUtensorMap tm[NUM_VARIANTS * MAPS];
+    memset(tm, 0, sizeof tm);
+    const void *bases[MAPS] = {p->mixed ? (const void *)p->r32 : (const void *)p->r64,
+                               p->mixed ? (const void *)p->pa32 : (const void *)p->pa64,
+                               p->mixed ? (const void *)p->pb32 : (const void *)p->pb64,
+                               (const void *)p->x,
+                               p->mixed ? (const void *)p->z32 : nullptr,
+                               p->mixed ? (const void *)p->ap32 : nullptr,
+                               p->mixed ? (const void *)p->ap32b : nullptr,
+                               nullptr};
+    for (int v = 0; v < NUM_VARIANTS; ++v) {
+        const Variant var = variant(p->mixed, v);
+        if (!var.fn) continue;
+        for (int q = 0; q < MAPS; ++q) {
+            // the fused pass's extra maps exist where its buffers do
+            if (q >= 4 && !bases[q]) continue;
+            if (!encode(&tm[MAPS * v + q], bases[q], q == 3 ? 8 : elem, nx, ny, nz, var.warps))
                 return (int)cudaErrorInvalidValue;
+        }
+    }
     if (!p->zc_maps) {
         cudaError_t e = cudaMalloc(&p->zc_maps, sizeof tm);
         if (e != cudaSuccess) return (int)e;
@@ -1140,6 +1405,9 @@ extern "C" int mbk_zcg_prepare(mb_pcg_dev *p) {
 extern "C" int mbk_zcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
     if (p->zc_variant < 0 || p->zc_variant >= NUM_VARIANTS || !p->zc_maps) return (int)cudaErrorInvalidValue;
     const Variant var = variant(p->mixed, p->zc_variant);
+    if (!var.fn) return (int)cudaErrorInvalidValue;
+    // the fused pass alternates r and A p between two buffers each
+    if (var.mode == FUSED && (!p->z32 || !p->ap32b)) return (int)cudaErrorInvalidValue;
     const int nx = p->st.nx, ny = p->st.ny, nz = p->st.nz;
     const int blocks = p->blocks;
     if (blocks <= 0) return (int)cudaErrorInvalidConfiguration;
@@ -1150,7 +1418,7 @@ extern "C" int mbk_zcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
     z.inv64 = p->zc_inv64;
     z.inv32 = p->zc_inv32;
     z.ptab32 = p->zc_ptab32;
-    z.maps = reinterpret_cast<const CUtensorMap *>(p->zc_maps) + 4 * p->zc_variant;
+    z.maps = reinterpret_cast<const CUtensorMap *>(p->zc_maps) + MAPS * p->zc_variant;
     z.tiles_x = (nx + TX - 1) / TX;
     z.tiles_y = (ny + var.warps - 1) / var.warps;
     z.by_gx = fastdiv((uint32_t)(nx / 4));
@@ -1174,7 +1442,7 @@ extern "C" int mbk_zcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
     a.x = p->x; a.vstar = p->vstar; a.b = p->b;
     a.r64 = p->r64; a.pa64 = p->pa64; a.pb64 = p->pb64; a.z64 = p->z64;
     a.r32 = p->r32; a.pa32 = p->pa32; a.pb32 = p->pb32; a.z32 = p->z32;
-    a.ap64 = p->ap64; a.ap32 = p->ap32;
+    a.ap64 = p->ap64; a.ap32 = p->ap32; a.ap32b = p->ap32b;
     a.inv_diag64 = p->inv_diag64; a.inv_diag32 = p->inv_diag32;
     a.partials = p->partials; a.ctrl = p->ctrl; a.bar = p->bar; a.status = p->status;
     cudaError_t e = cudaMemsetAsync(p->bar, 0, 2 * sizeof(unsigned), s);

@@ -185,9 +185,10 @@ typedef struct mb_pcg_dev {
     float *z32;
     double *ap64;            /* A p of the current direction (flat kernel) */
     float *ap32;
+    float *ap32b;            /* second A p buffer (z-march fused pass, mixed) */
     const double *inv_diag64;/* Jacobi 1/diag (FP64 form)   */
     const float *inv_diag32; /* Jacobi 1/diag (mixed form)  */
-    double *partials;        /* 2 * 4 * blocks */
+    double *partials;        /* 2 * 8 * blocks + 16 */
     mb_ctrl *ctrl;
     unsigned *bar;           /* 2 words, zero at start */
     int *status;             /* 0 = ok; set on a barrier timeout */

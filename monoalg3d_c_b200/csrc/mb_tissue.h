@@ -52,6 +52,7 @@ struct mb_monodomain {
     double *d_rtrue;             /* resident CG: FP64 true residual */
     double *d_ap;                /* flat CG: A p (FP64 form) */
     float *d_ap32;               /* flat CG: A p (mixed form) */
+    float *d_ap32b;              /* z-march fused pass: second A p buffer (mixed form) */
     unsigned *d_bar;
     int *d_status;
     float cg_tune_ms;     /* device time of one CG solve of the chosen kernel at tuning */

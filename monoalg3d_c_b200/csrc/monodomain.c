@@ -343,7 +343,7 @@ void mb_monodomain_destroy(mb_monodomain *m) {
     if (m->stream) cudaStreamSynchronize(m->stream);
     destroy_graphs(m);
     void *bufs[] = {m->d_pb, m->d_ppart, m->d_pb32, m->d_bar, m->d_status, m->d_invd, m->d_invd32, m->d_z, m->d_z32,
-                    m->d_rtrue, m->d_ap, m->d_ap32, m->d_ecg_leads, m->d_ecg_part, m->d_ecg_log,
+                    m->d_rtrue, m->d_ap, m->d_ap32, m->d_ap32b, m->d_ecg_leads, m->d_ecg_part, m->d_ecg_log,
                     m->d_mask, m->d_cells, m->d_v, m->d_vstar, m->d_r, m->d_p, m->d_r32, m->d_p32,
                     m->d_partials, m->d_sv64, m->d_sv32, m->d_stim_bits, m->d_celltype, m->d_scale,
                     m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_code, m->d_rowid, m->d_act,
@@ -823,8 +823,13 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
                 CKK(cudaMemset(m->d_z32, 0, (size_t)n * sizeof(float)));
                 ALLOC(m->d_ap32, (size_t)n * sizeof(float));
                 CKK(cudaMemset(m->d_ap32, 0, (size_t)n * sizeof(float)));
+                if (mbk_zcg_usable(&m->st)) {
+                    /* the z-march fused pass alternates A p between two buffers */
+                    ALLOC(m->d_ap32b, (size_t)n * sizeof(float));
+                    CKK(cudaMemset(m->d_ap32b, 0, (size_t)n * sizeof(float)));
+                }
             }
-            ALLOC(m->d_ppart, ((size_t)8 * blocks + 8) * sizeof(double));
+            ALLOC(m->d_ppart, ((size_t)16 * blocks + 16) * sizeof(double));
             if (d->precision == MB_PREC_FP64) {
                 ALLOC(m->d_invd, (size_t)n * sizeof(double));
                 CKK(cudaMemset(m->d_invd, 0, (size_t)n * sizeof(double)));
@@ -857,7 +862,7 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
             q->r64 = m->d_r; q->pa64 = m->d_p; q->pb64 = m->d_pb;
             q->r32 = m->d_r32; q->pa32 = m->d_p32; q->pb32 = m->d_pb32;
             q->z64 = m->d_z; q->z32 = m->d_z32;
-            q->ap64 = m->d_ap; q->ap32 = m->d_ap32;
+            q->ap64 = m->d_ap; q->ap32 = m->d_ap32; q->ap32b = m->d_ap32b;
             q->partials = m->d_ppart;
             q->inv_diag64 = m->d_invd;
             q->inv_diag32 = m->d_invd32;
