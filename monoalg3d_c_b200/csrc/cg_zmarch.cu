@@ -44,6 +44,7 @@
 // still in flight and leave the kernel; the other blocks then time out at
 // their next grid reduction and leave too.
 #include <cuda.h>
+#include <cstdlib>
 #include <cstring>
 #include "cg_common.cuh"
 
@@ -83,6 +84,10 @@ struct ZArgs {
     // tensor maps of r, p (buffer a), p (buffer b) and x, in global memory
     const CUtensorMap *maps;
     int tiles_x, tiles_y, chunks;
+    // 1: each block walks its own share of the (tile, plane) pairs in
+    // tile-major order (balanced ranges, below); 0: blocks take units of
+    // whole z chunks in turn (the window Q pass's form)
+    int balanced;
     FastDiv by_gx, by_ny;          // n / (nx / 4), n / ny
 };
 
@@ -241,6 +246,13 @@ __device__ __forceinline__ T coef(const mb_stencil_dev &st, size_t idx) {
 struct Unit {
     int x0, y0, k0, k1;
 };
+
+// Tile t (x fastest) over planes k0..k1-1.
+template <int W>
+__device__ __forceinline__ Unit tile_unit(const ZArgs &z, int t, int k0, int k1) {
+    const int ty = t / z.tiles_x;
+    return Unit{(t - ty * z.tiles_x) * TX, ty * W, k0, k1};
+}
 
 template <int W>
 __device__ __forceinline__ Unit unit_of(const ZArgs &z, int nz, int u) {
@@ -457,9 +469,7 @@ __device__ __forceinline__ bool zpass(const ZArgs &z, const Args &a, unsigned ch
     unsigned char *stage0 = smem + 128 + tabs_bytes;
     unsigned char *ring0 = stage0 + (size_t)S * stage_bytes;
     const int nz = a.st.nz;
-    const int units = z.tiles_x * z.tiles_y * z.chunks;
-    for (int un = blockIdx.x; un < units; un += gridDim.x) {
-        const Unit U = unit_of<W>(z, nz, un);
+    auto run = [&](const Unit &U) -> bool {
         const int P = U.k1 - U.k0 + 2;     // planes k0-1 .. k1
         if (threadIdx.x == 0) {
             fence_proxy_async();
@@ -500,7 +510,33 @@ __device__ __forceinline__ bool zpass(const ZArgs &z, const Args &a, unsigned ch
             }
         }
         __syncthreads();
+        return true;
+    };
+    if (z.balanced) {
+        // Block b walks the pairs [b N / G, (b + 1) N / G) of the N = tiles x nz
+        // (tile, plane) pairs in tile-major order, so every block has the same
+        // number of planes (within one) plus two halo planes per tile it
+        // touches.  Its tiles are walked last first: the block that ends a
+        // tile's range starts at plane 0 of the next tile, so every tile's
+        // plane k is reached within nz - N / G steps of step k and the halo
+        // rows neighbouring tiles share are still read from L2.
+        const long long N = (long long)z.tiles_x * z.tiles_y * nz;
+        const long long s0 = (long long)blockIdx.x * N / gridDim.x;
+        const long long s1 = (long long)(blockIdx.x + 1) * N / gridDim.x;
+        if (s1 > s0) {
+            const int tf = (int)(s0 / nz), tl = (int)((s1 - 1) / nz);
+            for (int t = tl; t >= tf; --t) {
+                const long long base = (long long)t * nz;
+                const int k0 = s0 > base ? (int)(s0 - base) : 0;
+                const int k1 = s1 < base + nz ? (int)(s1 - base) : nz;
+                if (!run(tile_unit<W>(z, t, k0, k1))) return false;
+            }
+        }
+        return true;
     }
+    const int units = z.tiles_x * z.tiles_y * z.chunks;
+    for (int un = blockIdx.x; un < units; un += gridDim.x)
+        if (!run(unit_of<W>(z, nz, un))) return false;
     return true;
 }
 
@@ -1436,6 +1472,18 @@ extern "C" int mbk_zcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
             }
         }
         z.chunks = bc;
+        // balanced ranges: planes per block plus two halo planes for each
+        // tile a range can touch; the window Q pass walks units only.
+        // MB_ZCG_SCHEDULE=chunks|balanced overrides the choice (tuning).
+        const long long pairs = (long long)z.tiles_x * z.tiles_y * nz;
+        const long long per = (pairs + blocks - 1) / blocks;
+        const long long bal = per + 2 * ((per + nz - 1) / nz + 1);
+        z.balanced = var.mode != QWIN && bal < best;
+        const char *env = getenv("MB_ZCG_SCHEDULE");
+        if (env && var.mode != QWIN) {
+            if (!strcmp(env, "chunks")) z.balanced = 0;
+            else if (!strcmp(env, "balanced")) z.balanced = 1;
+        }
     }
     Args a;
     a.st = p->st;
