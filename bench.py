@@ -174,19 +174,21 @@ class ClockSampler:
 #   (workload, cg kernel id) -> DRAM bytes (dram__bytes_read.sum +
 #   dram__bytes_write.sum) per active cell and CG iteration of one launch
 PROFILED_CG_TRAFFIC = {
-    # k_zcg<1, 8, 3, 2> on the 0.72-scale slab (360x360x72, every vector
-    # larger than L2): 6.445 GB over 9.33 M cells x 15 iterations
-    ("slab_500x500x100_torord_rotating_fibres", 301): 46.0,
+    # one-pass captures (dram__bytes_read.sum + dram__bytes_write.sum) of the
+    # full 25 M-cell slab's first solve after tuning, 15 iterations:
+    # k_zcg<1, 8, 3, 2, 2> 17.17 GB, k_zcg<1, 4, 3, 3, 2> 17.40 GB
+    ("slab_500x500x100_torord_rotating_fibres", 307): 45.8,
+    ("slab_500x500x100_torord_rotating_fibres", 309): 46.4,
 }
 #   (workload, "mixed" | "fp64", ode variant) -> pipe utilisation and MUFU
 #   (XU pipe) warp instructions x 32 per cell-step of one launch
 PROFILED_ODE = {
     # k_torord_mixed<0, 4> / k_torord_fp64<0, 3> on the 0.72-scale slab
     ("slab_500x500x100_torord_rotating_fibres", "mixed", 3): {
-        "xu_pct": 43.6, "fma_pct": 28.8, "fp64_pct": 1.1, "dram_bytes_per_cell_step": 411.6,
+        "xu_pct": 48.9, "fma_pct": 34.7, "fp64_pct": 1.2, "dram_bytes_per_cell_step": 411.7,
         "mufu_per_cell_step": 227.0},
     ("slab_500x500x100_torord_rotating_fibres", "fp64", 2): {
-        "fp64_pipe_pct": 18.5, "xu_pct": 4.7, "issue_active_pct": 22.1, "fp64_ops_per_cell_step": 3910.0,
+        "fp64_pipe_pct": 17.2, "xu_pct": 4.4, "issue_active_pct": 20.6, "fp64_ops_per_cell_step": 3912.0,
         "mufu_per_cell_step": 248.3},
 }
 
