@@ -674,17 +674,21 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         auto out = [&](const Unit &U, int k, int ts, unsigned char *lo, unsigned char *mid, unsigned char *hi) {
             const int j = U.y0 + w, i0 = U.x0 + 4 * lane;
             if (j >= ny) return;                     // warp-uniform
+            const size_t g0 = (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * k);
+            // the right-hand side's cells, loaded before the product so that
+            // the global load's latency runs under it
+            V4<double> bv = {{0.0, 0.0, 0.0, 0.0}};
+            if (i0 < nx) bv = ld4(a.b ? a.b + g0 : a.vstar + g0);
             const double *ct = tab64 + ts * TSLOT;
             const V4<double> ax = apply27<double, W>(st, reinterpret_cast<const double *>(lo),
                                                      reinterpret_cast<const double *>(mid),
                                                      reinterpret_cast<const double *>(hi), ct, i0, j, w, lane);
             if (i0 >= nx) return;
-            const size_t g0 = (size_t)i0 + (size_t)nx * ((size_t)j + (size_t)ny * k);
             const T *iv = tabT(ts) + JOFF + axis_class(j, ny) * 3;
             V4<T> rv;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                const double bb = a.b ? a.b[g0 + e] : st.alpha * a.vstar[g0 + e];
+                const double bb = a.b ? bv.v[e] : st.alpha * bv.v[e];
                 const double r64 = bb - ax.v[e];
                 const T rt = (T)r64;
                 const T zz = pre ? mul_rn(iv[axis_class(i0 + e, nx)], rt) : rt;
