@@ -26,14 +26,18 @@
 //
 // Each stage buffer and each ring plane is rewritten only after the block
 // barrier that follows its last use, so one __syncthreads per plane orders
-// the pipeline.  Blocks take units (x tile, y tile, z chunk) interleaved, so
-// the blocks of a round work on neighbouring tiles of the same planes and the
-// halo rows they share are read from L2.
+// the pipeline.  A block walks either an equal share of the (tile, plane)
+// pairs (balanced ranges) or units (x tile, y tile, z chunk) taken in turn;
+// either way the blocks work on neighbouring tiles at nearby planes and the
+// halo rows they share are mostly read from L2.
 //
-// Per iteration: Q (stencil pass: reads r, p_old; writes p, A p; p.Ap), then
-// U (streaming pass: x += alpha p, r -= alpha A p, r.z and r.r with z = r /
-// diag formed and dropped).  The FP64 residual b - A x (start and
-// refinements) is a stencil pass over x.  Jacobi 1/diag comes from a per-plane
+// Per iteration, ring and window forms: Q (stencil pass: reads r, p_old;
+// writes p, A p; p.Ap), then U (streaming pass: x += alpha p, r -= alpha A p,
+// r.z and r.r with z = r / diag formed and dropped).  Fused form (mixed):
+// one stencil pass that updates r from the staged r and A p, forms p, applies
+// the previous x update and sums seven products for one reduction (see
+// fpass).  The FP64 residual b - A x (start and refinements) is a stencil
+// pass over x.  Jacobi 1/diag comes from a per-plane
 // table of the nine row classes (1 / the class row's diagonal entry, the value
 // the flat kernel stores per cell).
 //
