@@ -89,3 +89,40 @@ def test_zmarch_mixed_matches_oracle_and_flat(reference, z):
     err = np.abs(got - ref)
     assert np.all(err <= 2e-3 * (np.abs(ref) + 1.0)), f"variant {z}: max |dV| {err.max():.3e}"
     assert np.abs(its - its_flat).max() <= 1
+
+
+@pytest.fixture(scope="module")
+def reference_plain_cg():
+    nx, ny, nz, kw = _case()
+    o = oracle.Sim(nx, ny, nz, use_preconditioner=False, **kw)
+    its = []
+    for _ in range(STEPS):
+        o.step(1)
+        its.append(o.last_cg()[0])
+    ref = o.v()
+    o.close()
+    return ref, np.array(its)
+
+
+@pytest.mark.parametrize("precision,z", [("fp64", 0), ("fp64", 2), ("mixed", 1), ("mixed", 7), ("mixed", 8),
+                                         ("mixed", 9)])
+def test_zmarch_without_preconditioner(reference_plain_cg, precision, z):
+    """The plain CG (use_preconditioner off: z = r, alpha = r.r / p.Ap, beta
+    from r.r) through the ring and fused forms: FP64 within 1e-8 relative
+    with the oracle's iteration counts, mixed within 2e-3 relative (+1 mV)
+    with iteration counts within one of the flat mixed kernel's."""
+    from monoalg3d_c_b200.monodomain import cg_launch_shapes
+    ref, its_ref = reference_plain_cg
+    nx, ny, nz, kw = _case()
+    kw = dict(kw, use_preconditioner=False)
+    nf = cg_launch_shapes()
+    kernel, got, its = _run(precision, nf + 2 + z, nx, ny, nz, kw)
+    assert kernel == 300 + z
+    err = np.abs(got - ref)
+    if precision == "fp64":
+        assert np.all(err <= 1e-8 * np.abs(ref) + 1e-9), f"variant {z}: max |dV| {err.max():.3e}"
+        assert np.array_equal(its, its_ref), f"variant {z}: CG iterations {its} vs oracle {its_ref}"
+    else:
+        _, _, its_flat = _run("mixed", 0, nx, ny, nz, kw)
+        assert np.all(err <= 2e-3 * (np.abs(ref) + 1.0)), f"variant {z}: max |dV| {err.max():.3e}"
+        assert np.abs(its - its_flat).max() <= 1
