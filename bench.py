@@ -1,7 +1,7 @@
 """Benchmark of the operator-split monodomain step (cell-steps/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--repeats R] [--config 4]
-                    [--impl ours|reference|reference-gpu]
+                    [--impl ours|reference|reference-gpu|reference-shim]
 
 A step is one iteration of the reference time loop (ODE sub-steps,
 update_monodomain, Jacobi-PCG to r.r <= 1e-16, clock) on the whole tissue.
@@ -30,6 +30,9 @@ GPU build (oracle/_ref/cuda: its host loop, its GPU cell-model kernels and
 its FP32 cuSPARSE/cuBLAS conjugate gradient) the same way, with the settings
 of its GPU examples (no preconditioner, tolerance 1e-16, at most 200
 iterations) -- the existing GPU code on the same GPU and tissue.
+--impl reference-shim times the drop-in: the reference's CPU build with this
+library's reference-host plugins (monoalg3d_c_b200/shim) as its cell model
+and linear solver, on the same tissue, by its own clocks.
 Under torchrun each rank runs an independent replica (the path does not shard:
 one GPU solves one tissue), so scaling is weak.
 """
@@ -62,7 +65,7 @@ def parse():
     ap.add_argument("--repeats", type=int, default=5)
     ap.add_argument("--config", type=int, default=4, choices=[0, 1, 2, 4])
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu", "reference-shim"])
     ap.add_argument("--ref-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the untimed activation-time comparison")
@@ -397,6 +400,33 @@ def reference_gpu_arm(args, wl, metric):
         "cg_iterations_per_step": r["cg_iterations"] / r["steps"]}))
 
 
+def reference_shim_arm(args, wl, metric):
+    """--impl reference-shim: the drop-in as a MonoAlg3D user gets it -- the
+    reference's own CPU build (its host loop, grid, assembly and
+    update_monodomain) with this library's reference-host plugins
+    (monoalg3d_c_b200/shim) named as its cell model and linear solver, on
+    the same tissue; the reference's own clocks."""
+    rr, case = reference_case(wl)
+    shim = os.path.join(REPO, "monoalg3d_c_b200", "shim", f"libmb_shim_{case['model']}.so")
+    if not rr.available() or not os.path.exists(shim):
+        print(json.dumps({"impl": "reference_shim", "unavailable": "the reference build (oracle/_ref) or the "
+                                                                   "shim plugins are not present"}))
+        return
+    r = reference_sample(rr, dict(case, plugin_lib=shim), max(args.ref_steps, 3))
+    v = r["cell_steps_per_s"]
+    print(json.dumps({
+        "impl": "reference_shim", "metric": metric, "value": v, "unit": "cell-steps/s", "n_gpus": 1,
+        "steps": r["steps"], "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl.name, "cells": wl.n, "active_cells": wl.active_cells(),
+                   "sampled_cells": int(r["cells"]), "same_tissue": bool(r["whole_tissue"])},
+        "settings": f"reference CPU build's host loop (oracle/_ref, {r['threads']} threads) with "
+                    f"{os.path.basename(shim)} as its cell model and linear solver (FP64 cell model and "
+                    "Jacobi-PCG on the GPU, tolerance 1e-16); its own clocks, Resolution Time - Total Write Time",
+        "phases_s": {"ode": r["ode_s"], "cg": r["cg_s"]},
+        "cg_iterations_per_step": r["cg_iterations"] / r["steps"]}))
+
+
 def main():
     args = parse()
     # at least 3 untimed warm-up steps, whatever was asked; the line reports
@@ -409,6 +439,10 @@ def main():
     if args.impl == "reference-gpu":
         if int(os.environ.get("RANK", "0")) == 0:
             reference_gpu_arm(args, workloads.CONFIGS[args.config](args.scale), metric)
+        return
+    if args.impl == "reference-shim":
+        if int(os.environ.get("RANK", "0")) == 0:
+            reference_shim_arm(args, workloads.CONFIGS[args.config](args.scale), metric)
         return
     if args.impl == "reference":
         # rank 0 alone runs the reference; no process group is needed

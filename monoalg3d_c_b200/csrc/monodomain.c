@@ -274,6 +274,12 @@ int mb_ode_set_steps(mb_ode *o, double dt, uint32_t num_steps) {
 int mb_ode_set_v(mb_ode *o, const double *v, size_t stride) {
     if (!o || !v || stride == 0) return set_err(MB_ERR_ARG, "bad arguments");
     const size_t n = o->dev.n;
+    if (stride == 1) {
+        /* contiguous: straight from the caller's buffer */
+        cudaError_t e = cudaMemcpyAsync(o->dev.sv64, v, n * sizeof(double), cudaMemcpyHostToDevice, o->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(o->stream);
+        return e == cudaSuccess ? MB_OK : set_err(MB_ERR_CUDA, "mb_ode_set_v: %s", cudaGetErrorString(e));
+    }
     double *tmp = (double *)malloc(n * sizeof(double));
     if (!tmp) return set_err(MB_ERR_NOMEM, "out of host memory");
     for (size_t i = 0; i < n; ++i) tmp[i] = v[i * stride];
@@ -286,6 +292,11 @@ int mb_ode_set_v(mb_ode *o, const double *v, size_t stride) {
 int mb_ode_get_v(mb_ode *o, double *v, size_t stride) {
     if (!o || !v || stride == 0) return set_err(MB_ERR_ARG, "bad arguments");
     const size_t n = o->dev.n;
+    if (stride == 1) {
+        cudaError_t e = cudaMemcpyAsync(v, o->dev.sv64, n * sizeof(double), cudaMemcpyDeviceToHost, o->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(o->stream);
+        return e == cudaSuccess ? MB_OK : set_err(MB_ERR_CUDA, "mb_ode_get_v: %s", cudaGetErrorString(e));
+    }
     double *tmp = (double *)malloc(n * sizeof(double));
     if (!tmp) return set_err(MB_ERR_NOMEM, "out of host memory");
     cudaError_t e = cudaMemcpyAsync(tmp, o->dev.sv64, n * sizeof(double), cudaMemcpyDeviceToHost, o->stream);

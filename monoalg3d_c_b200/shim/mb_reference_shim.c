@@ -76,6 +76,7 @@ static void shim_check(int rc, const char *what) {
 /* ---- cell-model library (ode_solver.h:33-47) ---------------------------- */
 
 static mb_ode *g_ode;        /* created at the first solve, when dt and num_steps are final */
+static double *g_vbuf;       /* V of every cell, contiguous (CPU-build entry points) */
 static uint32_t g_ode_cells;
 static uint8_t *g_celltype;  /* ToRORd cell type of every cell (extra data), or NULL */
 
@@ -149,13 +150,16 @@ SET_ODE_INITIAL_CONDITIONS_CPU(set_model_initial_conditions_cpu) {
     shim_check(mb_set_model_initial_conditions_gpu(tmp, NULL, g_celltype, &pitch), "initial conditions");
     shim_check(mb_ode_get_state(tmp, soa), "initial state");
     mb_ode_destroy(tmp);
-    for (uint32_t i = 0; i < n; ++i)
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i)
         for (int s = 0; s < neq; ++s) solver->sv[(size_t)i * neq + s] = soa[(size_t)s * n + i];
     free(soa);
     if (g_ode) {
         mb_ode_destroy(g_ode);
         g_ode = NULL;
     }
+    free(g_vbuf);
+    g_vbuf = NULL;
 }
 
 SOLVE_MODEL_ODES(solve_model_odes_cpu) {
@@ -169,7 +173,8 @@ SOLVE_MODEL_ODES(solve_model_odes_cpu) {
             fprintf(stderr, "monoalg3d_b200 shim: out of host memory\n");
             exit(1);
         }
-        for (uint32_t i = 0; i < n; ++i)
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)n; ++i)
             for (int s = 0; s < neq; ++s) soa[(size_t)s * n + i] = ode_solver->sv[(size_t)i * neq + s];
         shim_check(mb_ode_create(&g_ode, MB_SHIM_MODEL, MB_PREC_FP64, MB_RL_REFERENCE_CPU, n, ode_solver->min_dt,
                                  ode_solver->num_steps),
@@ -184,9 +189,25 @@ SOLVE_MODEL_ODES(solve_model_odes_cpu) {
         fprintf(stderr, "monoalg3d_b200 shim: the number of cells changed\n");
         exit(1);
     }
-    shim_check(mb_ode_set_v(g_ode, ode_solver->sv, (size_t)neq), "V upload");
+    /* V (every neq-th value of sv) through a contiguous buffer; the strided
+     * gather and scatter use the host's threads (the reference's own OpenMP
+     * team size) */
+    if (!g_vbuf) {
+        g_vbuf = (double *)malloc((size_t)n * sizeof(double));
+        if (!g_vbuf) {
+            fprintf(stderr, "monoalg3d_b200 shim: out of host memory\n");
+            exit(1);
+        }
+    }
+    const real *sv = ode_solver->sv;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) g_vbuf[i] = sv[(size_t)i * neq];
+    shim_check(mb_ode_set_v(g_ode, g_vbuf, 1), "V upload");
     shim_check(mb_solve_model_odes_gpu(g_ode, current_t, stim_currents), "solve_model_odes");
-    shim_check(mb_ode_get_v(g_ode, ode_solver->sv, (size_t)neq), "V download");
+    shim_check(mb_ode_get_v(g_ode, g_vbuf, 1), "V download");
+    real *svw = ode_solver->sv;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) svw[(size_t)i * neq] = g_vbuf[i];
 }
 
 /* ---- GPU build: the state lives on the device (ode_solver.h:37-47) -------- */
@@ -261,6 +282,10 @@ static void upload_matrix(uint32_t n, struct cell_node **cells) {
     int32_t *row_ptr = (int32_t *)malloc(((size_t)n + 1) * sizeof(int32_t));
     size_t nnz = 0;
     for (uint32_t i = 0; i < n; ++i) nnz += (size_t)arrlen(cells[i]->elements);
+    if (nnz > (size_t)INT32_MAX) {
+        fprintf(stderr, "monoalg3d_b200 shim: more than 2^31 - 1 matrix entries\n");
+        exit(1);
+    }
     int32_t *col = (int32_t *)malloc((nnz ? nnz : 1) * sizeof(int32_t));
     double *val = (double *)malloc((nnz ? nnz : 1) * sizeof(double));
     g_b = (double *)malloc((size_t)n * sizeof(double));
@@ -269,16 +294,16 @@ static void upload_matrix(uint32_t n, struct cell_node **cells) {
         fprintf(stderr, "monoalg3d_b200 shim: out of host memory\n");
         exit(1);
     }
-    size_t k = 0;
     row_ptr[0] = 0;
-    for (uint32_t i = 0; i < n; ++i) {
+    for (uint32_t i = 0; i < n; ++i) row_ptr[i + 1] = row_ptr[i] + (int32_t)arrlen(cells[i]->elements);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
         const struct element *el = cells[i]->elements;
-        const ptrdiff_t m = arrlen(cells[i]->elements);
-        for (ptrdiff_t e = 0; e < m; ++e, ++k) {
-            col[k] = (int32_t)el[e].column;
-            val[k] = el[e].value;
+        const int32_t k0 = row_ptr[i], m = row_ptr[i + 1] - k0;
+        for (int32_t e = 0; e < m; ++e) {
+            col[k0 + e] = (int32_t)el[e].column;
+            val[k0 + e] = el[e].value;
         }
-        row_ptr[i + 1] = (int32_t)k;
     }
     shim_check(mb_csr_create(&g_csr, (int32_t)n, row_ptr, col, val), "matrix upload");
     g_rows = n;
@@ -296,14 +321,18 @@ SOLVE_LINEAR_SYSTEM(conjugate_gradient) {
         fprintf(stderr, "monoalg3d_b200 shim: the matrix changed size (adaptivity is not supported)\n");
         exit(1);
     }
-    for (uint32_t i = 0; i < num_active_cells; ++i) {
+    /* b and the initial guess out of the host's cells, the solution back
+     * into them, on the host's threads */
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)num_active_cells; ++i) {
         g_b[i] = active_cells[i]->b;
         g_x[i] = active_cells[i]->v;
     }
     uint32_t its = 0;
     double err = 0.0;
     shim_check(mb_csr_solve(g_csr, g_b, g_x, g_tol, g_max_its, g_precond, &its, &err), "conjugate_gradient");
-    for (uint32_t i = 0; i < num_active_cells; ++i) active_cells[i]->v = g_x[i];
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)num_active_cells; ++i) active_cells[i]->v = g_x[i];
     *number_of_iterations = its;
     *error = err;
 }

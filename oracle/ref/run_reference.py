@@ -103,7 +103,9 @@ def ini_text(case: dict, work_dir: str, out_dir: str | None = None, dumps_every:
     save_state (dict: output_dir, save_rate) and restore_state (dict:
     input_dir) for the reference's checkpoint plugins, or None; dt_ode (ms,
     default dt); adaptive (bool, forward-Euler model "torord_endo") with
-    abs_tol, rel_tol."""
+    abs_tol, rel_tol; plugin_lib (a library file named in place of the stock
+    cell model and linear solver: the reference-host plugins of
+    monoalg3d_c_b200/shim)."""
     nx, ny, nz = case["nx"], case["ny"], case["nz"]
     dx = case.get("dx", 100.0)
     dt = case.get("dt", 0.02)
@@ -217,6 +219,12 @@ library_file={LIBS}/{MODEL_LIBS[case['model']]}
 """
     if case.get("use_gpu"):
         text = text.replace(f"library_file={LIBS}/", f"library_file={CUDA_LIBS}/")
+    if case.get("plugin_lib"):
+        # another library in place of the stock cell model and linear solver
+        # (the reference-host plugins of monoalg3d_c_b200/shim)
+        libs = CUDA_LIBS if case.get("use_gpu") else LIBS
+        for stock in (MODEL_LIBS[case["model"]], "libdefault_linear_system_solver.so"):
+            text = text.replace(f"library_file={libs}/{stock}", f"library_file={case['plugin_lib']}")
     return text
 
 
