@@ -126,3 +126,36 @@ def test_zmarch_without_preconditioner(reference_plain_cg, precision, z):
         _, _, its_flat = _run("mixed", 0, nx, ny, nz, kw)
         assert np.all(err <= 2e-3 * (np.abs(ref) + 1.0)), f"variant {z}: max |dV| {err.max():.3e}"
         assert np.abs(its - its_flat).max() <= 1
+
+
+@pytest.mark.parametrize("shape", [(8, 1, 1), (12, 3, 2), (136, 9, 3), (260, 17, 1)])
+def test_zmarch_small_and_ragged_grids(shape):
+    """Edge shapes of the tiling: the narrowest grid the kernel takes (8 cells
+    in x), one row, one plane, a last x tile of 4 or 8 cells, y tiles cut
+    short for every W.  The ring and fused shapes against the oracle (FP64
+    1e-8 relative with its iteration counts; mixed 2e-3 relative, +1 mV)."""
+    from monoalg3d_c_b200 import workloads
+    from monoalg3d_c_b200.monodomain import cg_launch_shapes
+    nx, ny, nz = shape
+    # fibres off the axes in every plane (one plane at 0 degrees would make
+    # the operator the plain 7-point one, which the z-march does not take)
+    kw = dict(model="torord", assembly="anisotropic", sigma_l=0.0002, sigma_t=0.00004, sigma_n=0.00004,
+              fibre_angle_z=np.deg2rad(np.linspace(45.0, -30.0, nz)),
+              celltype=workloads.transmural_thirds(nx, ny, nz), stims=[workloads.planar_stim()])
+    o = oracle.Sim(nx, ny, nz, **kw)
+    its_ref = []
+    for _ in range(STEPS):
+        o.step(1)
+        its_ref.append(o.last_cg()[0])
+    ref = o.v()
+    o.close()
+    nf = cg_launch_shapes()
+    for precision, z in (("fp64", 0), ("fp64", 2), ("mixed", 1), ("mixed", 7), ("mixed", 9)):
+        kernel, got, its = _run(precision, nf + 2 + z, nx, ny, nz, kw)
+        assert kernel == 300 + z, f"{shape} {precision} variant {z} not used ({kernel})"
+        err = np.abs(got - ref)
+        if precision == "fp64":
+            assert np.all(err <= 1e-8 * np.abs(ref) + 1e-9), f"{shape} variant {z}: max |dV| {err.max():.3e}"
+            assert np.array_equal(its, np.array(its_ref)), f"{shape} variant {z}: CG iterations differ"
+        else:
+            assert np.all(err <= 2e-3 * (np.abs(ref) + 1.0)), f"{shape} mixed variant {z}: max |dV| {err.max():.3e}"
