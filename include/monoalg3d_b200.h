@@ -389,7 +389,11 @@ int mb_reference_cell_order(int nx, int ny, int nz, const uint8_t *active, int64
  * when binary; cells in grid order.                                          */
 int mb_monodomain_save_v(mb_monodomain *m, const char *path, int binary);
 
-/* Device pointers to V (double, grid order) and to the CUDA stream used. */
+/* Device pointers to V (double, grid order) and to the CUDA stream used.
+ * V may be written through the pointer between steps (stream-ordered); the
+ * next mixed z-march solve, which otherwise starts from the product A x its
+ * previous solve stored, then takes more iterations to reach the same
+ * tolerance (mb_monodomain_set_v tells the tissue instead).               */
 int mb_monodomain_device_v(mb_monodomain *m, double **v_dev, void **stream);
 /* Average duration of the last kernel launches per kind, from CUDA events
  * recorded by mb_monodomain_profile_steps: ode, cg (whole solve). */

@@ -21,6 +21,7 @@ struct Args {
     double *ap64;              // A p of the current direction (stored by Q, read by U)
     float *ap32;
     float *ap32b;              // the z-march fused pass's second A p buffer
+    double *w;                 // the z-march fused solve's stored A x (FP64), or NULL
     const double *inv_diag64;  // Jacobi 1/diag per cell (FP64 form)
     const float *inv_diag32;   // Jacobi 1/diag per cell (mixed form)
     double *partials;          // 2 x 8 x gridDim.x partials

@@ -702,8 +702,44 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
                 acc[2] += r64 * r64;
             }
             st4(rdst + g0, rv);
+            // the fused solve keeps A x of its refinements: the last one is A x
+            // of the solution, the next solve's starting product
+            if (pk && a.w) st4(a.w + g0, ax);
         };
         return zpass<W, S>(z, a, smem, L::TABS, L::STAGE, L::RPLANE, pp, issue, tabs, form, out);
+    };
+
+    // ---- initial residual from the stored product (fused, mixed): r = b - w ----
+    // w = A x as the previous solve's last residual pass formed it for the x
+    // this solve starts from (the same FP64 sums), so r is the residual the
+    // stencil pass would give, for 20 streamed bytes per cell instead of a
+    // stencil pass.  Partials r.z, r.r, r64.r64 as there.
+    auto residual_w = [&](T *rdst, double (&acc)[3]) {
+        const unsigned gx = (unsigned)nx >> 2;
+        const unsigned groups = gx * (unsigned)ny * (unsigned)nz;
+        for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+            const size_t g0 = (size_t)q << 2;
+            const V4<double> bv = ld4(a.b ? a.b + g0 : a.vstar + g0);
+            const V4<double> wv = ld4(a.w + g0);
+            const unsigned t = z.by_gx.div(q);
+            const int i0 = (int)(q - t * gx) << 2;
+            const unsigned kk = z.by_ny.div(t);
+            const int k = (int)kk, j = (int)(t - kk * (unsigned)ny);
+            const T *irow = invt + k * 9 + axis_class(j, ny) * 3;
+            V4<T> rv;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const double bb = a.b ? bv.v[e] : st.alpha * bv.v[e];
+                const double r64 = bb - wv.v[e];
+                const T rt = (T)r64;
+                const T zz = pre ? mul_rn(__ldg(irow + axis_class(i0 + e, nx)), rt) : rt;
+                rv.v[e] = rt;
+                acc[0] += (double)rt * (double)zz;
+                acc[1] += (double)rt * (double)rt;
+                acc[2] += r64 * r64;
+            }
+            st4(rdst + g0, rv);
+        }
     };
 
     // ---- Q pass: p = r / diag + beta p_old, A p, p.Ap ------------------------------
@@ -1117,8 +1153,16 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         // is applied by the next fused pass, or by the residual pass's input
         // and then the final sweep below.
         double acc[3] = {0.0, 0.0, 0.0}, s3[3];
-        if (!residual(rbuf(0), nullptr, 0.0, acc)) return;
+        const bool wv = a.w != nullptr && c->w_valid != 0;
+        if (wv) residual_w(rbuf(0), acc);
+        else if (!residual(rbuf(0), nullptr, 0.0, acc)) return;
         if (!grid_reduce<3, 32 * W>(a, acc, s3, red)) return;
+        if (wv && !(s3[2] >= tol)) {
+            // the solve would stop here: decide on the stencil's residual
+            double t3[3] = {0.0, 0.0, 0.0};
+            if (!residual(rbuf(0), nullptr, 0.0, t3)) return;
+            if (!grid_reduce<3, 32 * W>(a, t3, s3, red)) return;
+        }
         double rz = s3[0], rr = s3[1];
         double error = s3[2], rr_ref = s3[2];
         int its = 1, refinements = 1;
@@ -1181,6 +1225,9 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
             c->refinements = refinements;
             c->rz = rz;
             c->rr = rr;
+            // w is A x of the solution when a refinement residual formed it, or
+            // when it was valid and x did not move
+            c->w_valid = (a.w != nullptr && (refinements > 1 || wv)) ? 1 : 0;
             c->done = 1;
         }
         return;
@@ -1251,6 +1298,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_zcg(Args a, ZArgs z) {
         c->refinements = refinements;
         c->rz = rz;
         c->rr = rr;
+        c->w_valid = 0;          // x moved without the fused solve's product
         c->done = 1;
     }
 }
@@ -1499,6 +1547,12 @@ extern "C" int mbk_zcg_launch(const mb_pcg_dev *p, cudaStream_t s) {
     a.r64 = p->r64; a.pa64 = p->pa64; a.pb64 = p->pb64; a.z64 = p->z64;
     a.r32 = p->r32; a.pa32 = p->pa32; a.pb32 = p->pb32; a.z32 = p->z32;
     a.ap64 = p->ap64; a.ap32 = p->ap32; a.ap32b = p->ap32b;
+    a.w = var.mode == FUSED ? p->zc_w : nullptr;
+    {
+        // MB_ZCG_STORED_PRODUCT=0: every solve starts with the stencil residual (tuning)
+        const char *env = getenv("MB_ZCG_STORED_PRODUCT");
+        if (env && !strcmp(env, "0")) a.w = nullptr;
+    }
     a.inv_diag64 = p->inv_diag64; a.inv_diag32 = p->inv_diag32;
     a.partials = p->partials; a.ctrl = p->ctrl; a.bar = p->bar; a.status = p->status;
     cudaError_t e = cudaMemsetAsync(p->bar, 0, 2 * sizeof(unsigned), s);

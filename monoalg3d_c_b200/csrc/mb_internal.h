@@ -54,6 +54,12 @@ typedef struct mb_ctrl {
     float   act_min_interval;/* ms between two counted activations          */
     /* pseudo-bidomain ECG */
     int64_t ecg_count;       /* records written                              */
+    /* z-march fused CG: 1 while the product A x the last solve stored (the
+     * tissue's zc_w) belongs to the current x; anything else that writes V
+     * clears it (a stale product costs iterations, never the answer: the
+     * stopping test is always on a residual from the stencil) */
+    int32_t w_valid;
+    int32_t pad_w_;
 } mb_ctrl;
 
 /* Structured grid, device view. */
@@ -206,6 +212,7 @@ typedef struct mb_pcg_dev {
     double *zc_inv64;
     float *zc_inv32;
     float *zc_ptab32;       /* [nz][mbk_zcg_ptab_floats()] per-plane blocks (window Q pass) */
+    double *zc_w;           /* A x of the fused solve's last residual (mixed), or NULL */
     void *zc_maps;
 } mb_pcg_dev;
 enum { MB_PCG_FLAT = 0, MB_PCG_TILED = 1, MB_PCG_RESIDENT = 2, MB_PCG_ZMARCH = 3 };

@@ -359,7 +359,7 @@ void mb_monodomain_destroy(mb_monodomain *m) {
                     m->d_partials, m->d_sv64, m->d_sv32, m->d_stim_bits, m->d_celltype, m->d_scale,
                     m->d_fx, m->d_fy, m->d_fz, m->d_table, m->d_table32, m->d_code, m->d_rowid, m->d_act,
                     m->d_stim_host, m->d_ctrl, m->d_log, m->d_stim2[0], m->d_stim2[1], m->d_vsnap[0],
-                    m->d_vsnap[1], m->pcg.zc_inv64, m->pcg.zc_inv32, m->pcg.zc_ptab32, m->pcg.zc_maps};
+                    m->d_vsnap[1], m->pcg.zc_inv64, m->pcg.zc_inv32, m->pcg.zc_ptab32, m->pcg.zc_maps, m->pcg.zc_w};
     for (size_t i = 0; i < sizeof bufs / sizeof bufs[0]; ++i) cudaFree(bufs[i]);
     for (int i = 0; i < 4; ++i) if (m->ev[i]) cudaEventDestroy(m->ev[i]);
     for (int i = 0; i < 4; ++i)
@@ -413,6 +413,12 @@ static int stim_covers(const mb_stim *s, const double c[3], int64_t g) {
 
 static int build_graphs(mb_monodomain *m);
 static int ode_autotune(mb_monodomain *m);
+
+/* V was written from outside the solve: the fused CG's stored A x no longer
+ * belongs to it (stream-ordered) */
+static void forget_stored_product(mb_monodomain *m) {
+    if (m->d_ctrl) cudaMemsetAsync(&m->d_ctrl->w_valid, 0, sizeof(int32_t), m->stream);
+}
 
 /* The start of a loop step: the ECG record of V_n when one is due
  * (monodomain_solver.c:654-657), then the cell models. */
@@ -493,6 +499,7 @@ static int cg_autotune(mb_monodomain *m) {
         float tsum = 0;
         for (int rep = 0; rep < 3 && !rc; ++rep) {
             cudaMemcpyAsync(m->d_v, vsave, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+            forget_stored_product(m);
             cudaEventRecord(m->ev[0], m->stream);
             const int e = pcg_launch(&q, m->stream);
             cudaEventRecord(m->ev[1], m->stream);
@@ -511,6 +518,7 @@ static int cg_autotune(mb_monodomain *m) {
         }
     }
     cudaMemcpyAsync(m->d_v, vsave, (size_t)m->n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream);
+    forget_stored_product(m);
     cudaStreamSynchronize(m->stream);
     cudaFree(vsave);
     if (rc) return rc;
@@ -853,6 +861,8 @@ int mb_monodomain_create(mb_monodomain **out, const mb_monodomain_desc *d) {
                 ALLOC(m->pcg.zc_inv64, (size_t)d->nz * 9 * sizeof(double));
                 ALLOC(m->pcg.zc_inv32, (size_t)d->nz * 9 * sizeof(float));
                 ALLOC(m->pcg.zc_ptab32, (size_t)d->nz * mbk_zcg_ptab_floats() * sizeof(float));
+                /* the fused mixed solve's stored A x (its next solve's starting product) */
+                if (d->precision == MB_PREC_MIXED) ALLOC(m->pcg.zc_w, (size_t)n * sizeof(double));
                 CKK(mbk_zcg_inv_tables(&m->st, m->pcg.zc_inv64, m->pcg.zc_inv32, m->pcg.zc_ptab32, m->stream));
             }
             CKK(cudaStreamSynchronize(m->stream));
@@ -1431,6 +1441,8 @@ int mb_monodomain_set_v(mb_monodomain *m, const double *v_host) {
     if (!m || !v_host) return set_err(MB_ERR_ARG, "null");
     CK(cudaStreamSynchronize(m->stream));
     CK(cudaMemcpy(m->d_v, v_host, (size_t)m->n * sizeof(double), cudaMemcpyHostToDevice));
+    forget_stored_product(m);
+    CK(cudaStreamSynchronize(m->stream));
     return MB_OK;
 }
 
@@ -1728,6 +1740,7 @@ int mb_tissue_snapshot(mb_monodomain *m, void *dev, int restore) {
                                 : cudaMemcpyAsync(snap, live[q], len[q], cudaMemcpyDeviceToDevice, m->stream);
         if (e != cudaSuccess) return set_err(MB_ERR_CUDA, "snapshot copy: %s", cudaGetErrorString(e));
     }
+    if (restore) forget_stored_product(m);
     return MB_OK;
 }
 
@@ -1813,6 +1826,10 @@ static int ckpt_copy(mb_monodomain *m, char *host, int restore) {
         char *p = host + base + mb_tissue_snapshot_bytes(m);
         if (restore) CK(cudaMemcpy(m->d_act, p, abytes, cudaMemcpyHostToDevice));
         else CK(cudaMemcpy(p, m->d_act, abytes, cudaMemcpyDeviceToHost));
+    }
+    if (restore) {
+        forget_stored_product(m);
+        CK(cudaStreamSynchronize(m->stream));
     }
     return MB_OK;
 }

@@ -471,6 +471,7 @@ int mb_monodomain_restore_state(mb_monodomain *m, const char *dir) {
         if (e == cudaSuccess) e = (cudaError_t)mbk_ode_scatter(&m->ode, dd, m->d_vstar, m->stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(m->d_v, v, (size_t)m->n * sizeof(double), cudaMemcpyHostToDevice,
                                                   m->stream);
+        c.w_valid = 0;           /* V comes from the file: no stored A x for it */
         if (e == cudaSuccess) e = cudaMemcpyAsync(m->d_ctrl, &c, sizeof c, cudaMemcpyHostToDevice, m->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
         cudaFree(dd);

@@ -159,3 +159,47 @@ def test_zmarch_small_and_ragged_grids(shape):
             assert np.array_equal(its, np.array(its_ref)), f"{shape} variant {z}: CG iterations differ"
         else:
             assert np.all(err <= 2e-3 * (np.abs(ref) + 1.0)), f"{shape} mixed variant {z}: max |dV| {err.max():.3e}"
+
+
+def test_fused_stored_product_and_outside_writes():
+    """The fused solve starts from the product A x that its previous solve's
+    last residual pass stored.  V written through the device pointer
+    (mb_monodomain_device_v), behind the library's back, leaves that product
+    stale: the next solve must still end on the stencil's own residual --
+    the same V as a tissue whose V was set through mb_monodomain_set_v (which
+    forgets the product) -- and only spend iterations on it."""
+    from cuda.bindings import runtime as rt
+    from monoalg3d_c_b200 import Tissue
+    from monoalg3d_c_b200.monodomain import cg_launch_shapes
+    nx, ny, nz, kw = _case()
+    old = os.environ.get("MB_CG_VARIANT")
+    try:
+        os.environ["MB_CG_VARIANT"] = str(cg_launch_shapes() + 2 + 7)
+        ta = Tissue(nx, ny, nz, precision="mixed", **kw)
+        tb = Tissue(nx, ny, nz, precision="mixed", **kw)
+    finally:
+        if old is None:
+            os.environ.pop("MB_CG_VARIANT", None)
+        else:
+            os.environ["MB_CG_VARIANT"] = old
+    assert ta.tuning()["cg_kernel"] == 307 and tb.tuning()["cg_kernel"] == 307
+    ta.step(20)
+    tb.step(20)
+    ta.sync()
+    tb.sync()
+    v = ta.v()
+    vmod = v.copy()
+    vmod[: nx * ny] += 5.0                        # the bottom plane 5 mV up
+    tb.set_v(vmod)
+    p, _ = ta.device_v()
+    err, = rt.cudaMemcpy(p, vmod.ctypes.data, vmod.nbytes, rt.cudaMemcpyKind.cudaMemcpyHostToDevice)
+    assert err == rt.cudaError_t.cudaSuccess
+    ta.step(5)
+    tb.step(5)
+    va, vb = ta.v(), tb.v()
+    sa, sb = ta.step_stats(20, 5), tb.step_stats(20, 5)
+    ta.close()
+    tb.close()
+    assert np.all(sa["error"] <= 1e-16) and np.all(sb["error"] <= 1e-16)
+    assert np.all(np.abs(va - vb) <= 1e-6 * (np.abs(vb) + 1.0)), f"max |dV| {np.abs(va - vb).max():.3e}"
+    assert sa["its"][0] >= sb["its"][0]
