@@ -303,25 +303,32 @@ __device__ __forceinline__ void load_row(const double *row, double (&cc)[CROW]) 
 // lo (k-1), mid (k), hi (k+1) (row stride WX, staged row h = the tile row +
 // 1) and the plane's class rows ct (9 rows of 27 entries in shared memory).
 // Every cell is first summed with the row of its y class and the interior x
-// class (the same row for the whole warp); lanes holding a cell on an x face
-// (i = 0 or nx - 1) then redo that cell with its own row.  Sums run in entry
-// order.  DENSE: every one of the 27 entries is applied -- the table holds
+// class (the same row for the whole warp); a cell on an x face (i = 0 or
+// nx - 1) is also summed with its own row, which replaces its first sum.
+// Sums run in entry order.  DENSE: every one of the 27 entries is applied -- the table holds
 // zeros where the operator has none, and fma(0, v, s) = s, so the sums are
 // those of the sparse form -- as straight-line code whose shared loads the
 // compiler can issue ahead of the arithmetic (measured faster than skipping
 // the entries that are zero in every row, st.nzmask, in both precisions).
 // All 32 lanes call it together.
-template <typename R, int W, bool DENSE = true>
-__device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, const R *mid, const R *hi,
-                                         const R *ct, int i0, int j, int w, int lane) {
-    const int cy = axis_class(j, st.ny);
+// FACE: some lane of the warp holds a cell on an x face (warp-uniform); its
+// own row's sum runs beside the others in the same entry order, from the
+// same values (the face cell's neighbours are already in the lane's
+// registers), instead of a pass over shared memory after them.
+template <typename R, int W, bool DENSE, bool FACE>
+__device__ __forceinline__ V4<R> apply27_rows(const mb_stencil_dev &st, const R *lo, const R *mid, const R *hi,
+                                              const R *ct, int e, int cy, int w, int lane) {
     const R *cm = ct + (cy * 3 + 1) * CROW;
+    // the face row of a lane holding a face cell (lanes without one read
+    // the low face's row and drop the sum)
+    const R *ce = ct + (cy * 3 + (e == 3 ? 2 : 0)) * CROW;
     const uint32_t mask = DENSE ? 0x7ffffffu : st.nzmask;
     // FP32: the row in registers, loaded as vectors; FP64 reads each entry
     // where it is used (its 28 values would take 56 registers)
     R cc[sizeof(R) == 4 ? CROW : 1];
     if constexpr (sizeof(R) == 4) load_row(cm, cc);
     R acc[4] = {R(0), R(0), R(0), R(0)};
+    R af = R(0);
     const int off = HX + 4 * lane;
     // the value beyond the tile's row: left of it for lane 0, right of it
     // for the others (used by lane 31) -- two distinct addresses in
@@ -357,31 +364,30 @@ __device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, 
                 else cq = cm[q];
 #pragma unroll
                 for (int c = 0; c < 4; ++c) acc[c] = fma(cq, wv[c + 1 + dx], acc[c]);
+                // the face cell (e = 0 or 3) and its neighbours e + dx
+                if constexpr (FACE) af = fma(ce[q], e == 3 ? wv[4 + dx] : wv[1 + dx], af);
             }
         }
     }
-    // cells on an x face: only the lanes holding one take this branch
-    const int e = i0 == 0 ? 0 : (i0 + 3 == st.nx - 1 ? 3 : -1);
-    if (e >= 0) {
-        const R *ce = ct + (cy * 3 + axis_class(i0 + e, st.nx)) * CROW;
-        R a = R(0);
-        for (int dz = -1; dz <= 1; ++dz) {
-            const R *pl = dz < 0 ? lo : (dz == 0 ? mid : hi);
-            for (int dy = -1; dy <= 1; ++dy) {
-                const R *rowp = pl + (w + 1 + dy) * WX + off + e;
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int q = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-                    if ((mask >> q) & 1u) a = fma(ce[q], rowp[dx], a);
-                }
-            }
-        }
-        if (e == 0) acc[0] = a;
-        else acc[3] = a;
+    if constexpr (FACE) {
+        if (e == 0) acc[0] = af;
+        else if (e == 3) acc[3] = af;
     }
     V4<R> out;
 #pragma unroll
     for (int c = 0; c < 4; ++c) out.v[c] = acc[c];
     return out;
+}
+
+template <typename R, int W, bool DENSE = true>
+__device__ __forceinline__ V4<R> apply27(const mb_stencil_dev &st, const R *lo, const R *mid, const R *hi,
+                                         const R *ct, int i0, int j, int w, int lane) {
+    const int cy = axis_class(j, st.ny);
+    // the lane's cell on an x face, if any: the first of its four on the
+    // low face, the last on the high face
+    const int e = i0 == 0 ? 0 : (i0 + 3 == st.nx - 1 ? 3 : -1);
+    if (__any_sync(0xffffffffu, e >= 0)) return apply27_rows<R, W, DENSE, true>(st, lo, mid, hi, ct, e, cy, w, lane);
+    return apply27_rows<R, W, DENSE, false>(st, lo, mid, hi, ct, e, cy, w, lane);
 }
 
 // The 27-point product for the lane's four cells of row j of plane k from a
