@@ -177,11 +177,10 @@ class ClockSampler:
 #   (workload, cg kernel id) -> DRAM bytes (dram__bytes_read.sum +
 #   dram__bytes_write.sum) per active cell and CG iteration of one launch
 PROFILED_CG_TRAFFIC = {
-    # one-pass captures (dram__bytes_read.sum + dram__bytes_write.sum) of the
-    # full 25 M-cell slab's first solve after tuning, 15 iterations:
-    # k_zcg<1, 8, 3, 2, 2> 17.17 GB, k_zcg<1, 4, 3, 3, 2> 17.40 GB
-    ("slab_500x500x100_torord_rotating_fibres", 307): 45.8,
-    ("slab_500x500x100_torord_rotating_fibres", 309): 46.4,
+    # one-pass capture (dram__bytes_read.sum + dram__bytes_write.sum) of the
+    # full 25 M-cell slab's second solve after tuning (the first to start
+    # from the stored product), 15 iterations: k_zcg<1, 8, 3, 2, 2> 16.46 GB
+    ("slab_500x500x100_torord_rotating_fibres", 307): 43.9,
 }
 #   (workload, "mixed" | "fp64", ode variant) -> pipe utilisation and MUFU
 #   (XU pipe) warp instructions x 32 per cell-step of one launch
